@@ -1,0 +1,47 @@
+// pac_backend.h -- what the plan layer needs from a device.
+//
+// The product library implements this interface on CUDA (pac_cuda.cu).
+// The test-only emulator (pac_emu.cpp, built as libpac_emu.so and loaded
+// only by tests/) implements it on host memory by replaying the same
+// pass_body phases on the CPU, so that the plan layer and the kernels' index
+// arithmetic can be checked without a GPU.
+#pragma once
+#include <stddef.h>
+
+#include "pac_engine.cuh"
+
+namespace pac {
+
+enum { CPY_H2D = 0, CPY_D2H = 1, CPY_D2D = 2 };
+
+int be_init();  // PAC_SUCCESS when a usable device is present
+int be_malloc(void** p, size_t bytes);
+int be_free(void* p);
+int be_memcpy(void* dst, const void* src, size_t bytes, int kind, void* stream);
+int be_memset(void* dst, int value, size_t bytes, void* stream);
+int be_stream_create(void** s);
+int be_stream_destroy(void* s);
+int be_stream_sync(void* s);
+int be_stream_wait(void* waiter, void* waitee);
+
+// one pass over `grid` CTAs (elem_bytes 8: double, 4: float; b2 = log2 base)
+int be_launch_pass(const PassDesc& d, int elem_bytes, int b2, long long grid, int threads,
+                   size_t smem, void* stream);
+// stage table (K = 2^logK, R = 2^logR): entry j*(R-1) + s-1 = w_K^{j s}, forward sign
+int be_fill_stage_tw(void* dst, int elem_bytes, int logK, int logR, void* stream);
+// dst[k] = w_N^{k * stride} for k < count, N = 2^logN, forward sign
+int be_fill_pow_tw(void* dst, int elem_bytes, long long count, long long stride, int logN,
+                   void* stream);
+// reference-layout tables of t levels for radix r (r^t - 1 entries)
+int be_fill_ref_tw(int r, int t, double* re, double* im, void* stream);
+int be_round_to_f32(const double* src, float* dst, long long n, void* stream);
+// y = scale * x .* h[i & hmask] (complex, split); elem_bytes 8 or 4
+int be_pointwise(long long n, int elem_bytes, const void* xr, const void* xi, const void* hr,
+                 const void* hi, long long hmask, void* yr, void* yi, double scale,
+                 void* stream);
+int be_scale_copy(long long n, int elem_bytes, const void* xr, const void* xi, void* yr,
+                  void* yi, double scale, void* stream);
+int be_permute(long long n, const int* rho, double* re, double* im, void* stream);
+long long be_launch_count();
+
+}  // namespace pac

@@ -1,0 +1,363 @@
+// pac_cuda.cu -- sm_100a kernels and the CUDA side of the plan layer.
+//
+// Kernels:
+//   pac_pass_kernel<T, B2>   one pass of the butterfly engine (pac_engine.cuh):
+//                            DIF / DIT / fused convolution, any radix schedule
+//   fill_*_tw                twiddle tables generated in FP64 with sincospi and
+//                            rounded once to the storage type
+//   pointwise, scale_copy, round_to_f32, permute   small elementwise kernels
+//
+// There is no host fallback: every entry point requires an sm_100 device and
+// fails with PAC_ERROR_NO_DEVICE otherwise.
+#include <cuda_runtime.h>
+#include <stdio.h>
+
+#include <atomic>
+#include <mutex>
+#include <set>
+#include <utility>
+
+#include "pac.h"
+#include "pac_backend.h"
+
+namespace pac {
+
+int set_error(int status, const char* fmt, ...);
+
+static std::atomic<long long> g_launches{0};
+
+static int cuda_fail(cudaError_t e, const char* what) {
+  return set_error(PAC_ERROR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+#define PAC_CU(call, what)                      \
+  do {                                          \
+    cudaError_t _e = (call);                    \
+    if (_e != cudaSuccess) return cuda_fail(_e, what); \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------------
+template <typename T, int B2>
+__global__ void __launch_bounds__(256) pac_pass_kernel(const PassDesc d) {
+  extern __shared__ __align__(16) unsigned char pac_smem[];
+  __shared__ long long s_lb[128];
+  T* sre = reinterpret_cast<T*>(pac_smem);
+  T* sim = sre + (size_t)d.W * d.pitch;
+  const long long cta = blockIdx.x;
+  if ((int)threadIdx.x < d.W) {
+    const int w = threadIdx.x;
+    const long long g = cta * d.W + w;
+    if (d.nat) {
+      nat_line<B2>(d, g, &s_lb[w], &s_lb[64 + w]);
+    } else {
+      s_lb[w] = line_base(d, g);
+      s_lb[64 + w] = s_lb[w];
+    }
+  }
+  __syncthreads();
+  pass_body<T, B2>(d, cta, sre, sim, s_lb, s_lb + 64);
+}
+
+template <typename T>
+__global__ void fill_stage_tw_kernel(Cx<T>* dst, int logK, int logR) {
+  const long long R1 = (1LL << logR) - 1;
+  const long long n = (1LL << (logK - logR)) * R1;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < n;
+       idx += (long long)gridDim.x * blockDim.x) {
+    long long j = idx / R1, s = idx % R1 + 1;
+    long long E = (j * s) & ((1LL << logK) - 1);
+    double x = -2.0 * (double)E / (double)(1LL << logK);
+    double sn, cs;
+    sincospi(x, &sn, &cs);
+    dst[idx] = Cx<T>{T(cs), T(sn)};
+  }
+}
+
+template <typename T>
+__global__ void fill_pow_tw_kernel(Cx<T>* dst, long long count, long long stride, int logN) {
+  const long long mask = (1LL << logN) - 1;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < count;
+       k += (long long)gridDim.x * blockDim.x) {
+    long long E = (k * stride) & mask;
+    double x = -2.0 * (double)E / (double)(1LL << logN);
+    double sn, cs;
+    sincospi(x, &sn, &cs);
+    dst[k] = Cx<T>{T(cs), T(sn)};
+  }
+}
+
+// reference layout: level q at offset r^q - 1, entry (m-1)*ell + j = w_k^{m j}
+__global__ void fill_ref_tw_kernel(int r, int t, double* re, double* im) {
+  long long total = 1;
+  for (int q = 0; q < t; ++q) total *= r;
+  total -= 1;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    long long ell = 1;
+    while (idx >= ell * r - 1) ell *= r;
+    long long local = idx - (ell - 1);
+    long long m = local / ell + 1, j = local % ell;
+    long long k = ell * r;
+    long long E = (m * j) % k;
+    double sn, cs;
+    sincospi(-2.0 * (double)E / (double)k, &sn, &cs);
+    re[idx] = cs;
+    im[idx] = sn;
+  }
+}
+
+__global__ void round_f32_kernel(const double* src, float* dst, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    dst[i] = (float)src[i];
+}
+
+template <typename T>
+__global__ void pointwise_kernel(long long n, const T* xr, const T* xi, const T* hr, const T* hi,
+                                 long long hmask, T* yr, T* yi, T scale) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    T ar = xr[i], ai = xi[i];
+    long long k = i & hmask;
+    T br = hr[k], bi = hi[k];
+    yr[i] = (ar * br - ai * bi) * scale;
+    yi[i] = (ar * bi + ai * br) * scale;
+  }
+}
+
+template <typename T>
+__global__ void scale_copy_kernel(long long n, const T* xr, const T* xi, T* yr, T* yi, T scale) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    yr[i] = xr[i] * scale;
+    yi[i] = xi[i] * scale;
+  }
+}
+
+// swap-based permutation by an involution (index_reversals.c:74-94); with
+// im == nullptr `re` holds interleaved (re, im) pairs
+__global__ void permute_kernel(long long n, const int* rho, double* re, double* im) {
+  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n;
+       j += (long long)gridDim.x * blockDim.x) {
+    long long p = rho[j];
+    if (j < p && p < n) {
+      if (im) {
+        double a = re[j], b = im[j];
+        re[j] = re[p];
+        im[j] = im[p];
+        re[p] = a;
+        im[p] = b;
+      } else {
+        double2* z = reinterpret_cast<double2*>(re);
+        double2 a = z[j];
+        z[j] = z[p];
+        z[p] = a;
+      }
+    }
+  }
+}
+
+static int grid_for(long long n) {
+  long long g = (n + 255) / 256;
+  if (g > 148 * 32) g = 148 * 32;
+  if (g < 1) g = 1;
+  return (int)g;
+}
+
+// ---------------------------------------------------------------------------
+// backend interface
+// ---------------------------------------------------------------------------
+int be_init() {
+  static std::once_flag once;
+  static int status = PAC_SUCCESS;
+  static char msg[256];
+  std::call_once(once, [] {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+      status = PAC_ERROR_NO_DEVICE;
+      snprintf(msg, sizeof(msg), "no CUDA device (%s)", cudaGetErrorString(e));
+      return;
+    }
+    int dev = 0, major = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+    if (major != 10) {
+      status = PAC_ERROR_NO_DEVICE;
+      snprintf(msg, sizeof(msg), "device %d is sm_%d0, this library is built for sm_100a", dev,
+               major);
+    }
+  });
+  if (status != PAC_SUCCESS) return set_error(status, "%s", msg);
+  return PAC_SUCCESS;
+}
+
+int be_malloc(void** p, size_t bytes) {
+  cudaError_t e = cudaMalloc(p, bytes ? bytes : 16);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return set_error(PAC_ERROR_ALLOC, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+  }
+  return PAC_SUCCESS;
+}
+
+int be_free(void* p) {
+  if (p) PAC_CU(cudaFree(p), "cudaFree");
+  return PAC_SUCCESS;
+}
+
+int be_memcpy(void* dst, const void* src, size_t bytes, int kind, void* stream) {
+  if (!bytes) return PAC_SUCCESS;
+  cudaMemcpyKind k = kind == CPY_H2D   ? cudaMemcpyHostToDevice
+                     : kind == CPY_D2H ? cudaMemcpyDeviceToHost
+                                       : cudaMemcpyDeviceToDevice;
+  PAC_CU(cudaMemcpyAsync(dst, src, bytes, k, (cudaStream_t)stream), "cudaMemcpyAsync");
+  return PAC_SUCCESS;
+}
+
+int be_memset(void* dst, int value, size_t bytes, void* stream) {
+  PAC_CU(cudaMemsetAsync(dst, value, bytes, (cudaStream_t)stream), "cudaMemsetAsync");
+  return PAC_SUCCESS;
+}
+
+int be_stream_create(void** s) {
+  cudaStream_t st;
+  PAC_CU(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate");
+  *s = st;
+  return PAC_SUCCESS;
+}
+int be_stream_destroy(void* s) {
+  if (s) PAC_CU(cudaStreamDestroy((cudaStream_t)s), "cudaStreamDestroy");
+  return PAC_SUCCESS;
+}
+int be_stream_sync(void* s) {
+  PAC_CU(cudaStreamSynchronize((cudaStream_t)s), "cudaStreamSynchronize");
+  return PAC_SUCCESS;
+}
+int be_stream_wait(void* waiter, void* waitee) {
+  cudaEvent_t ev;
+  PAC_CU(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "cudaEventCreate");
+  cudaError_t e = cudaEventRecord(ev, (cudaStream_t)waitee);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent((cudaStream_t)waiter, ev, 0);
+  cudaEventDestroy(ev);
+  if (e != cudaSuccess) return cuda_fail(e, "stream wait");
+  return PAC_SUCCESS;
+}
+
+template <typename T, int B2>
+static int launch_pass_t(const PassDesc& d, long long grid, int threads, size_t smem,
+                         void* stream) {
+  static std::mutex mu;
+  static std::set<std::pair<int, size_t>> configured;
+  auto kern = pac_pass_kernel<T, B2>;
+  if (smem > 48 * 1024) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> g(mu);
+    auto key = std::make_pair(dev, smem);
+    if (!configured.count(key)) {
+      PAC_CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+             "cudaFuncSetAttribute");
+      configured.insert(key);
+    }
+  }
+  if (grid > 0x7fffffffLL) return set_error(PAC_ERROR_SIZE, "pass grid too large");
+  kern<<<(unsigned)grid, threads, smem, (cudaStream_t)stream>>>(d);
+  PAC_CU(cudaGetLastError(), "pac_pass_kernel launch");
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return PAC_SUCCESS;
+}
+
+int be_launch_pass(const PassDesc& d, int elem_bytes, int b2, long long grid, int threads,
+                   size_t smem, void* stream) {
+  if (elem_bytes == 8) {
+    if (b2 == 1) return launch_pass_t<double, 1>(d, grid, threads, smem, stream);
+    if (b2 == 2) return launch_pass_t<double, 2>(d, grid, threads, smem, stream);
+    return launch_pass_t<double, 3>(d, grid, threads, smem, stream);
+  }
+  if (b2 == 1) return launch_pass_t<float, 1>(d, grid, threads, smem, stream);
+  if (b2 == 2) return launch_pass_t<float, 2>(d, grid, threads, smem, stream);
+  return launch_pass_t<float, 3>(d, grid, threads, smem, stream);
+}
+
+#define PAC_LAUNCHED(what)                  \
+  do {                                      \
+    PAC_CU(cudaGetLastError(), what);       \
+    g_launches.fetch_add(1);                \
+  } while (0)
+
+int be_fill_stage_tw(void* dst, int elem_bytes, int logK, int logR, void* stream) {
+  long long n = (1LL << (logK - logR)) * ((1LL << logR) - 1);
+  if (elem_bytes == 8)
+    fill_stage_tw_kernel<double><<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(
+        (Cx<double>*)dst, logK, logR);
+  else
+    fill_stage_tw_kernel<float><<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(
+        (Cx<float>*)dst, logK, logR);
+  PAC_LAUNCHED("fill_stage_tw");
+  return PAC_SUCCESS;
+}
+
+int be_fill_pow_tw(void* dst, int elem_bytes, long long count, long long stride, int logN,
+                   void* stream) {
+  if (elem_bytes == 8)
+    fill_pow_tw_kernel<double><<<grid_for(count), 256, 0, (cudaStream_t)stream>>>(
+        (Cx<double>*)dst, count, stride, logN);
+  else
+    fill_pow_tw_kernel<float><<<grid_for(count), 256, 0, (cudaStream_t)stream>>>(
+        (Cx<float>*)dst, count, stride, logN);
+  PAC_LAUNCHED("fill_pow_tw");
+  return PAC_SUCCESS;
+}
+
+int be_fill_ref_tw(int r, int t, double* re, double* im, void* stream) {
+  long long total = 1;
+  for (int q = 0; q < t; ++q) total *= r;
+  fill_ref_tw_kernel<<<grid_for(total), 256, 0, (cudaStream_t)stream>>>(r, t, re, im);
+  PAC_LAUNCHED("fill_ref_tw");
+  return PAC_SUCCESS;
+}
+
+int be_round_to_f32(const double* src, float* dst, long long n, void* stream) {
+  round_f32_kernel<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(src, dst, n);
+  PAC_LAUNCHED("round_f32");
+  return PAC_SUCCESS;
+}
+
+int be_pointwise(long long n, int elem_bytes, const void* xr, const void* xi, const void* hr,
+                 const void* hi, long long hmask, void* yr, void* yi, double scale,
+                 void* stream) {
+  if (elem_bytes == 8)
+    pointwise_kernel<double><<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(
+        n, (const double*)xr, (const double*)xi, (const double*)hr, (const double*)hi, hmask,
+        (double*)yr, (double*)yi, scale);
+  else
+    pointwise_kernel<float><<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(
+        n, (const float*)xr, (const float*)xi, (const float*)hr, (const float*)hi, hmask,
+        (float*)yr, (float*)yi, (float)scale);
+  PAC_LAUNCHED("pointwise");
+  return PAC_SUCCESS;
+}
+
+int be_scale_copy(long long n, int elem_bytes, const void* xr, const void* xi, void* yr,
+                  void* yi, double scale, void* stream) {
+  if (elem_bytes == 8)
+    scale_copy_kernel<double><<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(
+        n, (const double*)xr, (const double*)xi, (double*)yr, (double*)yi, scale);
+  else
+    scale_copy_kernel<float><<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(
+        n, (const float*)xr, (const float*)xi, (float*)yr, (float*)yi, (float)scale);
+  PAC_LAUNCHED("scale_copy");
+  return PAC_SUCCESS;
+}
+
+int be_permute(long long n, const int* rho, double* re, double* im, void* stream) {
+  permute_kernel<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(n, rho, re, im);
+  PAC_LAUNCHED("permute");
+  return PAC_SUCCESS;
+}
+
+long long be_launch_count() { return g_launches.load(); }
+
+}  // namespace pac

@@ -1,0 +1,208 @@
+// pac_emu.cpp -- TEST-ONLY host implementation of the backend interface.
+//
+// Built only into libpac_emu.so, which only tests/ load.  The product
+// library (libpac.so) never contains this file and has no host fallback.
+//
+// "Device" memory is host memory and a pass is replayed CTA by CTA, phase by
+// phase, through the same pass_body<T, B2> the sm_100a kernel runs, so the
+// plan layer, the pass geometry and the kernels' index arithmetic can be
+// checked against the oracle on a machine without a GPU.
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <atomic>
+#include <vector>
+
+#include "pac.h"
+#include "pac_backend.h"
+
+namespace pac {
+
+int set_error(int status, const char* fmt, ...);
+static std::atomic<long long> g_launches{0};
+
+int be_init() { return PAC_SUCCESS; }
+
+int be_malloc(void** p, size_t bytes) {
+  *p = aligned_alloc(256, ((bytes ? bytes : 16) + 255) / 256 * 256);
+  if (!*p) return set_error(PAC_ERROR_ALLOC, "host allocation failed");
+  return PAC_SUCCESS;
+}
+int be_free(void* p) {
+  free(p);
+  return PAC_SUCCESS;
+}
+int be_memcpy(void* dst, const void* src, size_t bytes, int, void*) {
+  if (bytes && dst != src) memmove(dst, src, bytes);
+  return PAC_SUCCESS;
+}
+int be_memset(void* dst, int value, size_t bytes, void*) {
+  memset(dst, value, bytes);
+  return PAC_SUCCESS;
+}
+int be_stream_create(void** s) {
+  *s = nullptr;
+  return PAC_SUCCESS;
+}
+int be_stream_destroy(void*) { return PAC_SUCCESS; }
+int be_stream_sync(void*) { return PAC_SUCCESS; }
+int be_stream_wait(void*, void*) { return PAC_SUCCESS; }
+
+template <typename T, int B2>
+static void replay(const PassDesc& d, long long grid) {
+  std::vector<T> sm((size_t)2 * d.W * d.pitch);
+  std::vector<long long> lb(128);
+  for (long long cta = 0; cta < grid; ++cta) {
+    for (int w = 0; w < d.W; ++w) {
+      long long g = cta * d.W + w;
+      if (d.nat) nat_line<B2>(d, g, &lb[w], &lb[64 + w]);
+      else lb[w] = lb[64 + w] = line_base(d, g);
+    }
+    pass_body<T, B2>(d, cta, sm.data(), sm.data() + (size_t)d.W * d.pitch, lb.data(),
+                     lb.data() + 64);
+  }
+}
+
+int be_launch_pass(const PassDesc& d, int elem_bytes, int b2, long long grid, int, size_t,
+                   void*) {
+  if (d.W > 64) return set_error(PAC_ERROR_INTERNAL, "W > 64");
+  if (elem_bytes == 8) {
+    if (b2 == 1) replay<double, 1>(d, grid);
+    else if (b2 == 2) replay<double, 2>(d, grid);
+    else replay<double, 3>(d, grid);
+  } else {
+    if (b2 == 1) replay<float, 1>(d, grid);
+    else if (b2 == 2) replay<float, 2>(d, grid);
+    else replay<float, 3>(d, grid);
+  }
+  g_launches++;
+  return PAC_SUCCESS;
+}
+
+// exp(-2 pi i E / N) evaluated in long double and rounded once
+static void root(long long E, long long N, double* c, double* s) {
+  long double a = -2.0L * 3.141592653589793238462643383279502884L * (long double)E / (long double)N;
+  *c = (double)cosl(a);
+  *s = (double)sinl(a);
+}
+
+template <typename T>
+static void put(void* dst, long long i, double c, double s) {
+  T* p = (T*)dst;
+  p[2 * i] = (T)c;
+  p[2 * i + 1] = (T)s;
+}
+
+int be_fill_stage_tw(void* dst, int elem_bytes, int logK, int logR, void*) {
+  long long R1 = (1LL << logR) - 1, K = 1LL << logK;
+  long long n = (K >> logR) * R1;
+  for (long long idx = 0; idx < n; ++idx) {
+    long long j = idx / R1, s = idx % R1 + 1;
+    double c, sn;
+    root((j * s) % K, K, &c, &sn);
+    if (elem_bytes == 8) put<double>(dst, idx, c, sn);
+    else put<float>(dst, idx, c, sn);
+  }
+  g_launches++;
+  return PAC_SUCCESS;
+}
+
+int be_fill_pow_tw(void* dst, int elem_bytes, long long count, long long stride, int logN, void*) {
+  long long N = 1LL << logN;
+  for (long long k = 0; k < count; ++k) {
+    double c, sn;
+    root((k * stride) & (N - 1), N, &c, &sn);
+    if (elem_bytes == 8) put<double>(dst, k, c, sn);
+    else put<float>(dst, k, c, sn);
+  }
+  g_launches++;
+  return PAC_SUCCESS;
+}
+
+int be_fill_ref_tw(int r, int t, double* re, double* im, void*) {
+  long long off = 0, ell = 1;
+  for (int q = 0; q < t; ++q) {
+    long long k = ell * r;
+    for (long long m = 1; m < r; ++m)
+      for (long long j = 0; j < ell; ++j) {
+        root((m * j) % k, k, &re[off + (m - 1) * ell + j], &im[off + (m - 1) * ell + j]);
+      }
+    off += (r - 1) * ell;
+    ell = k;
+  }
+  g_launches++;
+  return PAC_SUCCESS;
+}
+
+int be_round_to_f32(const double* src, float* dst, long long n, void*) {
+  for (long long i = 0; i < n; ++i) dst[i] = (float)src[i];
+  g_launches++;
+  return PAC_SUCCESS;
+}
+
+template <typename T>
+static void pointwise_t(long long n, const T* xr, const T* xi, const T* hr, const T* hi,
+                        long long hmask, T* yr, T* yi, T scale) {
+  for (long long i = 0; i < n; ++i) {
+    T ar = xr[i], ai = xi[i];
+    long long k = i & hmask;
+    T br = hr[k], bi = hi[k];
+    yr[i] = (ar * br - ai * bi) * scale;
+    yi[i] = (ar * bi + ai * br) * scale;
+  }
+}
+
+int be_pointwise(long long n, int elem_bytes, const void* xr, const void* xi, const void* hr,
+                 const void* hi, long long hmask, void* yr, void* yi, double scale, void*) {
+  if (elem_bytes == 8)
+    pointwise_t<double>(n, (const double*)xr, (const double*)xi, (const double*)hr,
+                        (const double*)hi, hmask, (double*)yr, (double*)yi, scale);
+  else
+    pointwise_t<float>(n, (const float*)xr, (const float*)xi, (const float*)hr, (const float*)hi,
+                       hmask, (float*)yr, (float*)yi, (float)scale);
+  g_launches++;
+  return PAC_SUCCESS;
+}
+
+int be_scale_copy(long long n, int elem_bytes, const void* xr, const void* xi, void* yr, void* yi,
+                  double scale, void*) {
+  for (long long i = 0; i < n; ++i) {
+    if (elem_bytes == 8) {
+      ((double*)yr)[i] = ((const double*)xr)[i] * scale;
+      ((double*)yi)[i] = ((const double*)xi)[i] * scale;
+    } else {
+      ((float*)yr)[i] = ((const float*)xr)[i] * (float)scale;
+      ((float*)yi)[i] = ((const float*)xi)[i] * (float)scale;
+    }
+  }
+  g_launches++;
+  return PAC_SUCCESS;
+}
+
+int be_permute(long long n, const int* rho, double* re, double* im, void*) {
+  for (long long j = 0; j < n; ++j) {
+    long long p = rho[j];
+    if (j < p && p < n) {
+      if (im) {
+        double a = re[j], b = im[j];
+        re[j] = re[p];
+        im[j] = im[p];
+        re[p] = a;
+        im[p] = b;
+      } else {
+        double a = re[2 * j], b = re[2 * j + 1];
+        re[2 * j] = re[2 * p];
+        re[2 * j + 1] = re[2 * p + 1];
+        re[2 * p] = a;
+        re[2 * p + 1] = b;
+      }
+    }
+  }
+  g_launches++;
+  return PAC_SUCCESS;
+}
+
+long long be_launch_count() { return g_launches.load(); }
+
+}  // namespace pac

@@ -1,0 +1,664 @@
+// pac_plan.cpp -- plans and pass schedules behind pac.h.
+//
+// A plan splits every axis of the problem into "virtual axes" (factors) no
+// longer than one CTA can hold in shared memory, and turns each operator
+// into a sequence of passes (one kernel launch each):
+//
+//   A^T  (forward):  DIF passes over the factors in memory order; the outer
+//                    factor of a split axis multiplies by the 4-step twiddle
+//                    w_N^{i * rev(e)} after its stages.  Output: P_b order.
+//   A, conj(A):      DIT passes in reverse order, 4-step twiddle before the
+//                    stages of an outer factor.  Input: P_b order.
+//   convolution:     DIF passes over all factors but the innermost, one fused
+//                    pass (DIF stages, product with the filter spectrum at the
+//                    same P_b positions, DIT stages) on the innermost factor,
+//                    then the DIT passes back.  2m-1 launches for m factors;
+//                    no pass ever permutes data in HBM.
+//   fft / ifft:      DIF passes whose last factor per axis stores in natural
+//                    order (self-sorting store of that pass).
+//
+// The reference performs the same factorisation with one stage per memory
+// sweep (butterflies.c) and per-axis gather/scatter (butterflies_2d.c,
+// butterflies_3d.c); the plan keeps its digit-reversal convention so the
+// spectrum order is the reference's P_r F x.
+#include <math.h>
+#include <stdarg.h>
+#include <stdlib.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <map>
+#include <memory>
+#include <mutex>
+#include <vector>
+
+#include "pac.h"
+#include "pac_backend.h"
+
+namespace pac {
+
+// ---------------------------------------------------------------------------
+// error reporting
+// ---------------------------------------------------------------------------
+static thread_local char t_err[512];
+
+int set_error(int status, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(t_err, sizeof(t_err), fmt, ap);
+  va_end(ap);
+  return status;
+}
+
+#define PAC_TRY(expr)                  \
+  do {                                 \
+    int _st = (expr);                  \
+    if (_st != PAC_SUCCESS) return _st; \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// schedules
+// ---------------------------------------------------------------------------
+struct VAx {
+  int log;      // factor length 2^log
+  int axis;     // real axis index
+  int first;    // first factor of its axis
+  int last;     // last (innermost) factor of its axis
+};
+
+struct Schedule {
+  int bytes = 8;  // element bytes of one real component
+  int b2 = 1;     // log2 of the digit base
+  std::vector<VAx> vax;
+  std::vector<std::vector<int>> rad;  // per factor: stage radix logs, DIF order
+  void* pool = nullptr;               // stage twiddle tables
+  std::map<std::pair<int, int>, int> tw_off;
+  struct Tw4 {
+    void* lo = nullptr;
+    void* hi = nullptr;
+    int lolog = 0;
+  };
+  std::map<int, Tw4> tw4;  // keyed by log N
+  ~Schedule() {
+    if (pool) be_free(pool);
+    for (auto& kv : tw4) {
+      be_free(kv.second.lo);
+      be_free(kv.second.hi);
+    }
+  }
+};
+
+static const int kSmemBudget = 200 * 1024;
+
+// stage radices of one factor of length 2^lg for digit base 2^b2
+static std::vector<int> radix_schedule(int lg, int b2) {
+  std::vector<int> r;
+  if (b2 == 3) {
+    for (int i = 0; i < lg; i += 3) r.push_back(3);
+  } else if (b2 == 2) {
+    int x = lg;
+    while (x >= 4) {
+      r.push_back(4);
+      x -= 4;
+    }
+    if (x) r.push_back(2);
+  } else {
+    int x = lg;
+    while (x >= 4) {
+      r.push_back(4);
+      x -= 4;
+    }
+    if (x) r.push_back(x);
+  }
+  return r;
+}
+
+// Longest factor one CTA holds: 2^12 complex FP64 / 2^13 complex FP32
+// (64 KiB per line).  PAC_MAX_FACTOR_LOG lowers it, which forces more
+// factors per axis (used by the tests to reach 3- and 4-factor splits at
+// small sizes).
+static int max_factor_log(int bytes, int b2) {
+  int lmax = bytes == 8 ? 12 : 13;
+  const char* env = getenv("PAC_MAX_FACTOR_LOG");
+  if (env) {
+    int v = atoi(env);
+    if (v >= b2 && v < lmax) lmax = v;
+  }
+  return lmax - lmax % b2;
+}
+
+static int build_schedule(Schedule& s, int rank, const int* logs, int b2, int bytes) {
+  s.bytes = bytes;
+  s.b2 = b2;
+  int lmax = max_factor_log(bytes, b2);
+  for (int a = 0; a < rank; ++a) {
+    int lg = logs[a];
+    if (lg == 0) continue;
+    int digits = lg / b2;
+    int dmax = lmax / b2;
+    int nf = (digits + dmax - 1) / dmax;
+    if (nf > PAC_MAX_FACTORS)
+      return set_error(PAC_ERROR_SIZE, "axis %d needs %d factors (at most %d)", a, nf,
+                       (int)PAC_MAX_FACTORS);
+    std::vector<int> parts(nf, digits / nf);
+    for (int i = 0; i < digits % nf; ++i) parts[nf - 1 - i]++;
+    for (int f = 0; f < nf; ++f) s.vax.push_back({parts[f] * b2, a, f == 0, f == nf - 1});
+  }
+  for (auto& v : s.vax) s.rad.push_back(radix_schedule(v.log, b2));
+  // stage twiddle tables
+  std::vector<std::pair<int, int>> specs;
+  long long total = 0;
+  for (size_t i = 0; i < s.vax.size(); ++i) {
+    int logK = s.vax[i].log;
+    for (int rl : s.rad[i]) {
+      std::pair<int, int> key(logK, rl);
+      if (!s.tw_off.count(key) && logK > rl) {
+        s.tw_off[key] = (int)total;
+        specs.push_back(key);
+        total += (1LL << (logK - rl)) * ((1LL << rl) - 1);
+      }
+      logK -= rl;
+    }
+  }
+  if (total > 0) {
+    PAC_TRY(be_malloc(&s.pool, (size_t)total * 2 * bytes));
+    for (auto& k : specs) {
+      char* dst = (char*)s.pool + (size_t)s.tw_off[k] * 2 * bytes;
+      PAC_TRY(be_fill_stage_tw(dst, bytes, k.first, k.second, nullptr));
+    }
+  }
+  // 4-step twiddles: for every non-last factor, N = L * (later factors of its axis)
+  for (size_t i = 0; i < s.vax.size(); ++i) {
+    if (s.vax[i].last) continue;
+    int logN = 0;
+    for (size_t j = i; j < s.vax.size() && s.vax[j].axis == s.vax[i].axis; ++j) logN += s.vax[j].log;
+    if (s.tw4.count(logN)) continue;
+    Schedule::Tw4 t;
+    t.lolog = (logN + 1) / 2;
+    long long nlo = 1LL << t.lolog, nhi = 1LL << (logN - t.lolog);
+    PAC_TRY(be_malloc(&t.lo, (size_t)nlo * 2 * bytes));
+    PAC_TRY(be_malloc(&t.hi, (size_t)nhi * 2 * bytes));
+    PAC_TRY(be_fill_pow_tw(t.lo, bytes, nlo, 1, logN, nullptr));
+    PAC_TRY(be_fill_pow_tw(t.hi, bytes, nhi, nlo, logN, nullptr));
+    s.tw4[logN] = t;
+  }
+  return PAC_SUCCESS;
+}
+
+}  // namespace pac
+
+// ---------------------------------------------------------------------------
+// the plan object
+// ---------------------------------------------------------------------------
+struct pac_plan_s {
+  int rank = 0;
+  int dims[3] = {1, 1, 1};
+  int logs[3] = {0, 0, 0};
+  long long batch = 1;
+  int b2 = 1;
+  int form = PAC_FORM_F64;
+  long long N = 1;
+  pac::Schedule main;                     // storage type of the form
+  std::unique_ptr<pac::Schedule> s64;     // FP64 schedule (F32 form: filter spectrum)
+  std::mutex ws_mu;
+  void* ws = nullptr;  // workspace: 2 arrays of batch*N elements of the storage type
+  size_t ws_bytes = 0;
+  void* tmp64 = nullptr;  // FP64 temporary for the F32 filter spectrum
+  size_t tmp64_bytes = 0;
+  ~pac_plan_s() {
+    if (ws) pac::be_free(ws);
+    if (tmp64) pac::be_free(tmp64);
+  }
+};
+
+namespace pac {
+
+struct PassSpec {
+  PassDesc d;
+  long long grid;
+  int threads;
+  size_t smem;
+  bool oop;  // cannot run in place
+};
+
+// geometry of a pass over factor vi for `batch` problems
+static PassSpec make_pass(const Schedule& s, int vi, long long batch, long long N) {
+  PassSpec p;
+  PassDesc& d = p.d;
+  memset(&d, 0, sizeof(d));
+  const VAx& v = s.vax[vi];
+  const int esz = s.bytes;
+  const int SH = esz == 8 ? 4 : 5, NB = esz == 8 ? 16 : 32;
+  d.L = 1 << v.log;
+  d.logL = v.log;
+  int logS = 0;
+  for (size_t j = vi + 1; j < s.vax.size(); ++j) logS += s.vax[j].log;
+  d.logS = logS;
+  d.nlines = (batch * N) >> v.log;
+  const int base_pitch = d.L + (d.L >> SH);
+  long long target = (esz == 8 ? 4096 : 8192) >> v.log;
+  long long W = target < 1 ? 1 : target;
+  if (logS > 0) {
+    if (W < 16) W = 16;
+    if (W > (1LL << logS)) W = 1LL << logS;
+  }
+  long long wmax = kSmemBudget / (2LL * esz * (base_pitch + NB));
+  if (wmax < 1) wmax = 1;
+  while (W > wmax) W >>= 1;
+  if (W > 64) W = 64;
+  while (W > d.nlines) W >>= 1;
+  if (W < 1) W = 1;
+  d.W = (int)W;
+  d.logW = 0;
+  while ((1 << d.logW) < d.W) ++d.logW;
+  int pitch = base_pitch;
+  if (d.W > 1) {
+    int want = (NB / (d.W < NB ? d.W : NB)) % NB;
+    pitch += ((want - pitch % NB) % NB + NB) % NB;
+  }
+  d.pitch = pitch;
+  const std::vector<int>& rad = s.rad[vi];
+  d.nst = (int)rad.size();
+  int logK = v.log;
+  int min_rl = 4;
+  for (int i = 0; i < d.nst; ++i) {
+    d.rlog[i] = rad[i];
+    auto it = s.tw_off.find(std::make_pair(logK, rad[i]));
+    d.tw_off[i] = it == s.tw_off.end() ? 0 : it->second;
+    logK -= rad[i];
+    if (rad[i] < min_rl) min_rl = rad[i];
+  }
+  d.tw = s.pool;
+  long long bf = (long long)d.W << (v.log - 4 > 0 ? v.log - 4 : 0);
+  int threads = (int)(bf < 32 ? 32 : bf > 256 ? 256 : bf);
+  threads = (threads + 31) / 32 * 32;
+  d.nthreads = threads;
+  if (!v.last) {
+    int logGin = 0, logSreal = 0;
+    for (size_t j = vi + 1; j < s.vax.size(); ++j) {
+      if (s.vax[j].axis == v.axis) logGin += s.vax[j].log;
+      else logSreal += s.vax[j].log;
+    }
+    int logN = v.log + logGin;
+    auto& t = s.tw4.at(logN);
+    d.tw4_shift = logSreal;
+    d.tw4_mask = (1LL << logGin) - 1;
+    d.tw4_lolog = t.lolog;
+    d.tw4_lo = t.lo;
+    d.tw4_hi = t.hi;
+  }
+  p.grid = d.nlines / d.W;
+  p.threads = threads;
+  p.smem = (size_t)2 * d.W * d.pitch * esz;
+  p.oop = false;
+  return p;
+}
+
+static int launch(const Schedule& s, PassSpec& p, void* stream) {
+  return be_launch_pass(p.d, s.bytes, s.b2, p.grid, p.threads, p.smem, stream);
+}
+
+static int get_ws(pac_plan_s* pl, size_t bytes, void** out) {
+  if (pl->ws_bytes < bytes) {
+    if (pl->ws) be_free(pl->ws);
+    pl->ws = nullptr;
+    pl->ws_bytes = 0;
+    PAC_TRY(be_malloc(&pl->ws, bytes));
+    pl->ws_bytes = bytes;
+  }
+  *out = pl->ws;
+  return PAC_SUCCESS;
+}
+
+// Run one operator of schedule s over `batch` problems.
+static int run_transform(pac_plan_s* pl, const Schedule& s, int op, long long batch,
+                         const void* in_re, const void* in_im, void* out_re, void* out_im,
+                         double scale, int use_scale, void* stream) {
+  const long long N = pl->N;
+  const int m = (int)s.vax.size();
+  const long long total = batch * N;
+  if (m == 0) {
+    double sc = use_scale ? scale : 1.0;
+    return be_scale_copy(total, s.bytes, in_re, in_im, out_re, out_im, sc, stream);
+  }
+  std::vector<PassSpec> passes;
+  if (op == PAC_OP_AT || op == PAC_OP_FFT || op == PAC_OP_IFFT) {
+    int sign = (op == PAC_OP_IFFT) ? +1 : -1;
+    for (int vi = 0; vi < m; ++vi) {
+      PassSpec p = make_pass(s, vi, batch, N);
+      p.d.mode = MODE_DIF;
+      p.d.sign = sign;
+      p.d.tw4 = s.vax[vi].last ? 0 : 1;
+      if (op != PAC_OP_AT && s.vax[vi].last) {
+        // natural-order store of this axis
+        p.d.nat = 1;
+        int nf = 0, Mlog = 0;
+        for (int j = vi - 1; j >= 0 && s.vax[j].axis == s.vax[vi].axis; --j) ++nf;
+        for (int f = 0; f < nf; ++f) {
+          p.d.nat_flog[f] = s.vax[vi - nf + f].log;
+          Mlog += s.vax[vi - nf + f].log;
+        }
+        p.d.nat_nf = nf;
+        p.d.nat_Mlog = Mlog;
+        p.oop = nf > 0;
+      }
+      passes.push_back(p);
+    }
+  } else {
+    int sign = (op == PAC_OP_A || op == PAC_OP_UFFT) ? -1 : +1;
+    for (int vi = m - 1; vi >= 0; --vi) {
+      PassSpec p = make_pass(s, vi, batch, N);
+      p.d.mode = MODE_DIT;
+      p.d.sign = sign;
+      p.d.tw4 = s.vax[vi].last ? 0 : 2;
+      passes.push_back(p);
+    }
+  }
+  if (use_scale) {
+    passes.back().d.use_scale = 1;
+    passes.back().d.scale = scale;
+  }
+  // buffer sequence: the last pass must write `out`
+  const size_t arr_bytes = (size_t)total * s.bytes;
+  int flips = 0;
+  for (size_t i = 1; i < passes.size(); ++i) flips += passes[i].oop ? 1 : 0;
+  void* ws = nullptr;
+  bool need_ws = flips > 0 || (passes[0].oop && in_re == out_re);
+  std::unique_lock<std::mutex> lk(pl->ws_mu, std::defer_lock);
+  if (need_ws) {
+    lk.lock();
+    PAC_TRY(get_ws(pl, 2 * arr_bytes, &ws));
+  }
+  void* bre[2] = {out_re, ws};
+  void* bim[2] = {out_im, ws ? (char*)ws + arr_bytes : nullptr};
+  int cur = (flips % 2 == 0) ? 0 : 1;
+  if (passes[0].oop && in_re == bre[cur]) cur ^= 1;  // only when in == out
+  const void* src_re = in_re;
+  const void* src_im = in_im;
+  for (size_t i = 0; i < passes.size(); ++i) {
+    PassSpec& p = passes[i];
+    int dst = cur;
+    if (i > 0 && p.oop) dst = cur ^ 1;
+    p.d.in_re = src_re;
+    p.d.in_im = src_im;
+    p.d.out_re = bre[dst];
+    p.d.out_im = bim[dst];
+    PAC_TRY(launch(s, p, stream));
+    cur = dst;
+    src_re = bre[cur];
+    src_im = bim[cur];
+  }
+  if (cur != 0) PAC_TRY(be_memcpy(out_re, bre[cur], arr_bytes, CPY_D2D, stream));
+  if (cur != 0) PAC_TRY(be_memcpy(out_im, bim[cur], arr_bytes, CPY_D2D, stream));
+  return PAC_SUCCESS;
+}
+
+static int run_conv(pac_plan_s* pl, const void* x_re, const void* x_im, const void* h_re,
+                    const void* h_im, int per_problem, void* y_re, void* y_im, double scale,
+                    void* stream) {
+  const Schedule& s = pl->main;
+  const long long N = pl->N;
+  const int m = (int)s.vax.size();
+  const long long hmask = per_problem ? -1LL : (N - 1);
+  if (m == 0)
+    return be_pointwise(pl->batch * N, s.bytes, x_re, x_im, h_re, h_im, hmask, y_re, y_im, scale,
+                        stream);
+  for (int vi = 0; vi < m - 1; ++vi) {
+    PassSpec p = make_pass(s, vi, pl->batch, N);
+    p.d.mode = MODE_DIF;
+    p.d.sign = -1;
+    p.d.tw4 = s.vax[vi].last ? 0 : 1;
+    p.d.in_re = vi == 0 ? x_re : y_re;
+    p.d.in_im = vi == 0 ? x_im : y_im;
+    p.d.out_re = y_re;
+    p.d.out_im = y_im;
+    PAC_TRY(launch(s, p, stream));
+  }
+  {
+    PassSpec p = make_pass(s, m - 1, pl->batch, N);
+    p.d.mode = MODE_CONV;
+    p.d.h_re = h_re;
+    p.d.h_im = h_im;
+    p.d.h_mask = hmask;
+    p.d.scale = scale;
+    p.d.in_re = m == 1 ? x_re : y_re;
+    p.d.in_im = m == 1 ? x_im : y_im;
+    p.d.out_re = y_re;
+    p.d.out_im = y_im;
+    PAC_TRY(launch(s, p, stream));
+  }
+  for (int vi = m - 2; vi >= 0; --vi) {
+    PassSpec p = make_pass(s, vi, pl->batch, N);
+    p.d.mode = MODE_DIT;
+    p.d.sign = +1;
+    p.d.tw4 = s.vax[vi].last ? 0 : 2;
+    p.d.in_re = y_re;
+    p.d.in_im = y_im;
+    p.d.out_re = y_re;
+    p.d.out_im = y_im;
+    PAC_TRY(launch(s, p, stream));
+  }
+  return PAC_SUCCESS;
+}
+
+}  // namespace pac
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+using namespace pac;
+
+static int ilog2_exact(long long v, int b2) {
+  if (v < 1) return -1;
+  int lg = 0;
+  while ((1LL << lg) < v) ++lg;
+  if ((1LL << lg) != v) return -1;
+  if (lg % b2) return -1;
+  return lg;
+}
+
+extern "C" {
+
+PAC_API int pac_plan_create(pac_plan_t* plan, int rank, const int* dims, int batch,
+                            int digit_base, int form) {
+  if (!plan || !dims || rank < 1 || rank > 3 || batch < 1)
+    return set_error(PAC_ERROR_INVALID_VALUE, "pac_plan_create: invalid rank/dims/batch");
+  if (digit_base == 0) digit_base = 2;
+  int b2 = digit_base == 2 ? 1 : digit_base == 4 ? 2 : digit_base == 8 ? 3 : 0;
+  if (!b2)
+    return set_error(PAC_ERROR_UNSUPPORTED_RADIX, "pac_plan_create: digit base %d not in {2,4,8}",
+                     digit_base);
+  if (form != PAC_FORM_F64 && form != PAC_FORM_F32)
+    return set_error(PAC_ERROR_INVALID_VALUE, "pac_plan_create: unknown form %d", form);
+  int st = be_init();
+  if (st != PAC_SUCCESS) return st;
+  std::unique_ptr<pac_plan_s> p(new pac_plan_s());
+  p->rank = rank;
+  p->batch = batch;
+  p->b2 = b2;
+  p->form = form;
+  long long N = 1;
+  for (int a = 0; a < rank; ++a) {
+    int lg = ilog2_exact(dims[a], b2);
+    if (lg < 0)
+      return set_error(PAC_ERROR_NOT_POWER, "pac_plan_create: axis %d length %d is not a power of %d",
+                       a, dims[a], digit_base);
+    p->dims[a] = dims[a];
+    p->logs[a] = lg;
+    N *= dims[a];
+  }
+  if (N * (long long)batch > (1LL << 40) || N > (1LL << 31))
+    return set_error(PAC_ERROR_SIZE, "pac_plan_create: problem too large");
+  p->N = N;
+  int bytes = form == PAC_FORM_F64 ? 8 : 4;
+  st = build_schedule(p->main, rank, p->logs, b2, bytes);
+  if (st != PAC_SUCCESS) return st;
+  if (bytes != 8) {
+    p->s64.reset(new Schedule());
+    st = build_schedule(*p->s64, rank, p->logs, b2, 8);
+    if (st != PAC_SUCCESS) return st;
+  }
+  *plan = p.release();
+  return PAC_SUCCESS;
+}
+
+PAC_API int pac_plan_destroy(pac_plan_t plan) {
+  delete plan;
+  return PAC_SUCCESS;
+}
+
+PAC_API int pac_plan_get_info(pac_plan_t plan, pac_plan_info_t* info) {
+  if (!plan || !info) return set_error(PAC_ERROR_INVALID_VALUE, "pac_plan_get_info: NULL");
+  memset(info, 0, sizeof(*info));
+  info->n_elements = plan->N;
+  info->batch = plan->batch;
+  info->rank = plan->rank;
+  for (int a = 0; a < 3; ++a) info->dims[a] = plan->dims[a];
+  info->digit_base = 1 << plan->b2;
+  info->form = plan->form;
+  info->element_bytes = plan->main.bytes;
+  int m = (int)plan->main.vax.size();
+  info->conv_passes = m == 0 ? 1 : 2 * m - 1;
+  info->transform_passes = m == 0 ? 1 : m;
+  info->workspace_bytes = plan->ws_bytes + plan->tmp64_bytes;
+  return PAC_SUCCESS;
+}
+
+PAC_API int pac_filter_spectrum(pac_plan_t plan, const double* h_re, const double* h_im,
+                                int nfilters, void* hhat_re, void* hhat_im, double scale,
+                                pac_stream_t stream) {
+  if (!plan || !h_re || !h_im || !hhat_re || !hhat_im)
+    return set_error(PAC_ERROR_INVALID_VALUE, "pac_filter_spectrum: NULL argument");
+  if (nfilters != 1 && nfilters != plan->batch)
+    return set_error(PAC_ERROR_INVALID_VALUE, "pac_filter_spectrum: nfilters must be 1 or batch");
+  if (plan->form == PAC_FORM_F64)
+    return run_transform(plan, plan->main, PAC_OP_AT, nfilters, h_re, h_im, hhat_re, hhat_im, scale,
+                         1, stream);
+  // F32 form: FP64 transform into a temporary, rounded once
+  std::lock_guard<std::mutex> g(plan->ws_mu);
+  size_t need = (size_t)nfilters * plan->N * 2 * sizeof(double);
+  if (plan->tmp64_bytes < need) {
+    if (plan->tmp64) be_free(plan->tmp64);
+    plan->tmp64 = nullptr;
+    plan->tmp64_bytes = 0;
+    PAC_TRY(be_malloc(&plan->tmp64, need));
+    plan->tmp64_bytes = need;
+  }
+  double* tre = (double*)plan->tmp64;
+  double* tim = tre + (size_t)nfilters * plan->N;
+  // the FP64 schedule never needs the workspace for A^T
+  PAC_TRY(run_transform(plan, *plan->s64, PAC_OP_AT, nfilters, h_re, h_im, tre, tim, scale, 1,
+                        stream));
+  PAC_TRY(be_round_to_f32(tre, (float*)hhat_re, (long long)nfilters * plan->N, stream));
+  PAC_TRY(be_round_to_f32(tim, (float*)hhat_im, (long long)nfilters * plan->N, stream));
+  return PAC_SUCCESS;
+}
+
+PAC_API int pac_convolve(pac_plan_t plan, const void* x_re, const void* x_im, const void* hhat_re,
+                         const void* hhat_im, int hhat_per_problem, void* y_re, void* y_im,
+                         double scale, pac_stream_t stream) {
+  if (!plan || !x_re || !x_im || !hhat_re || !hhat_im || !y_re || !y_im)
+    return set_error(PAC_ERROR_INVALID_VALUE, "pac_convolve: NULL argument");
+  return run_conv(plan, x_re, x_im, hhat_re, hhat_im, hhat_per_problem ? 1 : 0, y_re, y_im, scale,
+                  stream);
+}
+
+PAC_API int pac_transform(pac_plan_t plan, int op, const void* in_re, const void* in_im,
+                          void* out_re, void* out_im, pac_stream_t stream) {
+  if (!plan || !in_re || !in_im || !out_re || !out_im)
+    return set_error(PAC_ERROR_INVALID_VALUE, "pac_transform: NULL argument");
+  if (op < PAC_OP_AT || op > PAC_OP_UIFFT)
+    return set_error(PAC_ERROR_INVALID_VALUE, "pac_transform: unknown op %d", op);
+  bool scaled = op == PAC_OP_IFFT || op == PAC_OP_UIFFT;
+  return run_transform(plan, plan->main, op, plan->batch, in_re, in_im, out_re, out_im,
+                       scaled ? 1.0 / (double)plan->N : 1.0, scaled ? 1 : 0, stream);
+}
+
+PAC_API int pac_pointwise_product(long long n, const double* x_re, const double* x_im,
+                                  const double* h_re, const double* h_im, double* y_re,
+                                  double* y_im, double scale, pac_stream_t stream) {
+  if (n < 0 || (n > 0 && (!x_re || !x_im || !h_re || !h_im || !y_re || !y_im)))
+    return set_error(PAC_ERROR_INVALID_VALUE, "pac_pointwise_product: bad argument");
+  if (n == 0) return PAC_SUCCESS;
+  PAC_TRY(be_init());
+  return be_pointwise(n, 8, x_re, x_im, h_re, h_im, -1LL, y_re, y_im, scale, stream);
+}
+
+PAC_API int pac_scale(long long n, const double* x_re, const double* x_im, double* y_re,
+                      double* y_im, double scale, pac_stream_t stream) {
+  if (n < 0 || (n > 0 && (!x_re || !x_im || !y_re || !y_im)))
+    return set_error(PAC_ERROR_INVALID_VALUE, "pac_scale: bad argument");
+  if (n == 0) return PAC_SUCCESS;
+  PAC_TRY(be_init());
+  return be_scale_copy(n, 8, x_re, x_im, y_re, y_im, scale, stream);
+}
+
+PAC_API int pac_permute(long long n, const int* rho, double* re, double* im, pac_stream_t stream) {
+  if (n < 0 || (n > 0 && (!rho || !re)))
+    return set_error(PAC_ERROR_INVALID_VALUE, "pac_permute: bad argument");
+  if (n == 0) return PAC_SUCCESS;
+  PAC_TRY(be_init());
+  return be_permute(n, rho, re, im, stream);
+}
+
+PAC_API int pac_reference_twiddles(int r, int n, double* re, double* im, pac_stream_t stream) {
+  if ((r != 2 && r != 4 && r != 8) || n < 1 || !re || !im)
+    return set_error(PAC_ERROR_INVALID_VALUE, "pac_reference_twiddles: bad argument");
+  PAC_TRY(be_init());
+  // the reference's level count (twiddle_factors.c:18, :40-45, :77-82)
+  int t = 0;
+  if (r == 2) {
+    while (!((n >> t) & 1)) ++t;
+  } else {
+    int sh = r == 4 ? 2 : 3;
+    for (int v = n; v > 1; v >>= sh) ++t;
+  }
+  if (t == 0) return PAC_SUCCESS;
+  return be_fill_ref_tw(r, t, re, im, stream);
+}
+
+PAC_API int pac_malloc(void** ptr, size_t bytes) {
+  if (!ptr) return set_error(PAC_ERROR_INVALID_VALUE, "pac_malloc: NULL");
+  PAC_TRY(be_init());
+  return be_malloc(ptr, bytes);
+}
+PAC_API int pac_free(void* ptr) { return ptr ? be_free(ptr) : PAC_SUCCESS; }
+PAC_API int pac_memcpy_h2d(void* dst, const void* src, size_t bytes, pac_stream_t s) {
+  return be_memcpy(dst, src, bytes, CPY_H2D, s);
+}
+PAC_API int pac_memcpy_d2h(void* dst, const void* src, size_t bytes, pac_stream_t s) {
+  return be_memcpy(dst, src, bytes, CPY_D2H, s);
+}
+PAC_API int pac_memcpy_d2d(void* dst, const void* src, size_t bytes, pac_stream_t s) {
+  return be_memcpy(dst, src, bytes, CPY_D2D, s);
+}
+PAC_API int pac_stream_create(pac_stream_t* s) {
+  if (!s) return set_error(PAC_ERROR_INVALID_VALUE, "pac_stream_create: NULL");
+  PAC_TRY(be_init());
+  return be_stream_create(s);
+}
+PAC_API int pac_stream_destroy(pac_stream_t s) { return be_stream_destroy(s); }
+PAC_API int pac_stream_synchronize(pac_stream_t s) { return be_stream_sync(s); }
+PAC_API int pac_stream_wait_stream(pac_stream_t waiter, pac_stream_t waitee) {
+  return be_stream_wait(waiter, waitee);
+}
+PAC_API long long pac_launch_count(void) { return be_launch_count(); }
+
+PAC_API const char* pac_status_string(int status) {
+  switch (status) {
+    case PAC_SUCCESS: return "success";
+    case PAC_ERROR_INVALID_VALUE: return "invalid value";
+    case PAC_ERROR_NOT_POWER: return "axis length is not a power of the radix";
+    case PAC_ERROR_UNSUPPORTED_RADIX: return "unsupported radix";
+    case PAC_ERROR_SIZE: return "problem too large";
+    case PAC_ERROR_CUDA: return "CUDA error";
+    case PAC_ERROR_NO_DEVICE: return "no usable sm_100 device";
+    case PAC_ERROR_ALLOC: return "allocation failed";
+    case PAC_ERROR_TIMEOUT: return "device wait timed out";
+    default: return "internal error";
+  }
+}
+
+PAC_API const char* pac_last_error(void) { return t_err; }
+
+}  // extern "C"

@@ -1,0 +1,180 @@
+/*
+ * pac.h -- native C ABI of the B200 permutation-avoiding FFT convolution.
+ *
+ * Plain C: opaque plan handles, device pointers, sizes and int status codes.
+ * The reference (venkovic/c-permutation-avoiding-convolution) has no plan
+ * object and no device API; every entry point below states which reference
+ * function(s) it stands in for.  The reference-compatible host-pointer
+ * entry points (identical prototypes) are declared in fft.h and are built
+ * on top of this header.
+ *
+ * Data layout (the reference's): split complex arrays -- one array of real
+ * parts, one of imaginary parts -- row-major with the last axis contiguous
+ * (butterflies_3d.c:24-26).  A plan covers `batch` independent problems
+ * stored back to back.
+ *
+ * Spectrum order: the forward stages leave the spectrum of every axis in
+ * base-b digit-reversed order P_b (b = the plan's digit base), exactly as
+ * the reference's transposed butterflies do (A^T x = P_b F x).  With b equal
+ * to the reference radix r the order is bit-identical to the reference's.
+ *
+ * Forms: PAC_FORM_F64 computes and stores complex FP64.  PAC_FORM_F32 stores
+ * and computes FP32, with twiddles and the filter spectrum computed in FP64
+ * on the device and rounded once.
+ *
+ * Threading: plans are immutable after creation; calls on one plan from
+ * several host threads are safe when they use distinct buffers (the plan's
+ * workspace is locked internally).  All device work is asynchronous on the
+ * given stream unless stated otherwise.
+ */
+#ifndef PAC_H
+#define PAC_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define PAC_API __attribute__((visibility("default")))
+#else
+#define PAC_API
+#endif
+
+typedef struct pac_plan_s* pac_plan_t;
+typedef void* pac_stream_t; /* a cudaStream_t; NULL is the legacy default stream */
+
+/* status codes */
+enum {
+  PAC_SUCCESS = 0,
+  PAC_ERROR_INVALID_VALUE = 1,     /* NULL pointer, bad rank/batch/op      */
+  PAC_ERROR_NOT_POWER = 2,         /* an axis length is not a power of b   */
+  PAC_ERROR_UNSUPPORTED_RADIX = 3, /* digit base / radix not supported     */
+  PAC_ERROR_SIZE = 4,              /* problem larger than the int index range */
+  PAC_ERROR_CUDA = 5,              /* a CUDA runtime call failed           */
+  PAC_ERROR_NO_DEVICE = 6,         /* no usable sm_100 device              */
+  PAC_ERROR_ALLOC = 7,             /* device or host allocation failed     */
+  PAC_ERROR_TIMEOUT = 8,           /* a bounded device wait gave up        */
+  PAC_ERROR_INTERNAL = 9
+};
+
+/* storage / compute forms */
+enum { PAC_FORM_F64 = 0, PAC_FORM_F32 = 1 };
+
+/* transform operators (per axis, all axes of the plan) */
+enum {
+  PAC_OP_AT = 0,      /* x <- A^T x = P_b F x      apply_transposed_butterflies_r* */
+  PAC_OP_A = 1,       /* x <- A x   = F P_b x      apply_butterflies_r*            */
+  PAC_OP_CONJ_A = 2,  /* x <- conj(A) x            apply_conjugate_butterflies_r*  */
+  PAC_OP_FFT = 3,     /* natural -> natural F x    fft, fft2                       */
+  PAC_OP_IFFT = 4,    /* natural -> natural F^-1 x ifft                            */
+  PAC_OP_UFFT = 5,    /* = PAC_OP_A                ufft                            */
+  PAC_OP_UIFFT = 6    /* conj(A) x / N             uifft                           */
+};
+
+typedef struct {
+  long long n_elements;   /* elements of one problem (product of dims)    */
+  long long batch;
+  int rank;
+  int dims[3];
+  int digit_base;
+  int form;
+  int element_bytes;      /* bytes of one real component (8 or 4)        */
+  int conv_passes;        /* kernel launches of one pac_convolve          */
+  int transform_passes;   /* kernel launches of one forward transform     */
+  size_t workspace_bytes; /* device workspace held by the plan            */
+} pac_plan_info_t;
+
+/* Plan for `batch` problems of shape dims[0..rank-1] (rank 1..3).  Every
+ * axis length must be a power of digit_base (2, 4 or 8); digit_base 0 picks
+ * 2.  Allocates the twiddle tables on the current device.
+ * Stands in for precompute_twiddles_r{2,4,8} (twiddle_factors.c:17,39,76):
+ * the tables are generated on the device in FP64. */
+PAC_API int pac_plan_create(pac_plan_t* plan, int rank, const int* dims, int batch,
+                            int digit_base, int form);
+/* free_twiddles (twiddle_factors.c:133) */
+PAC_API int pac_plan_destroy(pac_plan_t plan);
+PAC_API int pac_plan_get_info(pac_plan_t plan, pac_plan_info_t* info);
+
+/* Filter spectrum: hhat = scale * A^T h, P_b order, computed in FP64 and
+ * rounded once to the plan's storage type.  h_re/h_im are FP64 device
+ * arrays of nfilters problems (1, or the plan's batch); hhat has the plan's
+ * element type.  In place (h == hhat) is allowed for PAC_FORM_F64.
+ * The reference recomputes this inside every call
+ * (convolution.c:45-53); the plan API computes it once. */
+PAC_API int pac_filter_spectrum(pac_plan_t plan, const double* h_re, const double* h_im,
+                                int nfilters, void* hhat_re, void* hhat_im, double scale,
+                                pac_stream_t stream);
+
+/* Circular convolution of every problem of the batch:
+ *   y = conj(A)[ scale * (A^T x) .* hhat ]
+ * hhat from pac_filter_spectrum; hhat_per_problem = 0 applies one filter
+ * spectrum to every problem, 1 reads one spectrum per problem.  x may alias
+ * y.  permutation_avoiding_convolution{,_2d,_3d} (convolution.c:31,
+ * convolution_2d.c:35, convolution_3d.c:36) with the filter transform
+ * hoisted into the plan. */
+PAC_API int pac_convolve(pac_plan_t plan, const void* x_re, const void* x_im,
+                         const void* hhat_re, const void* hhat_im, int hhat_per_problem,
+                         void* y_re, void* y_im, double scale, pac_stream_t stream);
+
+/* One operator over all axes of every problem, in -> out (may alias).
+ * See PAC_OP_*.  For PAC_OP_FFT / PAC_OP_IFFT an axis split over several
+ * passes needs the plan workspace (allocated on first use). */
+PAC_API int pac_transform(pac_plan_t plan, int op, const void* in_re, const void* in_im,
+                          void* out_re, void* out_im, pac_stream_t stream);
+
+/* y = scale * x .* h elementwise over n complex FP64 values (the product
+ * loop of convolution.c:55-62 on its own; the reference's convolution
+ * reduces to it when the radix is not supported). */
+PAC_API int pac_pointwise_product(long long n, const double* x_re, const double* x_im,
+                                  const double* h_re, const double* h_im, double* y_re,
+                                  double* y_im, double scale, pac_stream_t stream);
+
+/* y = scale * x elementwise over n complex FP64 values (the division by n
+ * of ifft / uifft, fft.c:69-70, on its own). x may alias y. */
+PAC_API int pac_scale(long long n, const double* x_re, const double* x_im, double* y_re,
+                      double* y_im, double scale, pac_stream_t stream);
+
+/* Swap x[j] <-> x[rho[j]] for j < rho[j], rho an involution
+ * (apply_permutation_split, index_reversals.c:85; apply_permutation,
+ * index_reversals.c:74).  rho is a device int array of n entries.  With
+ * im == NULL, re is an interleaved complex array of n (re, im) pairs. */
+PAC_API int pac_permute(long long n, const int* rho, double* re, double* im,
+                        pac_stream_t stream);
+
+/* Stage twiddles in the reference layout (twiddle_factors.c:17-131):
+ * level q (k = r^(q+1), ell = k/r) has (r-1)*ell entries, entry
+ * (m-1)*ell + j = exp(-2 pi i m j / k).  Writes all levels back to back
+ * into the device arrays re/im ((n-1) entries in total). */
+PAC_API int pac_reference_twiddles(int r, int n, double* re, double* im, pac_stream_t stream);
+
+/* Device memory and streams (thin wrappers so that C callers need no CUDA
+ * headers). */
+PAC_API int pac_malloc(void** ptr, size_t bytes);
+PAC_API int pac_free(void* ptr);
+PAC_API int pac_memcpy_h2d(void* dst, const void* src, size_t bytes, pac_stream_t stream);
+PAC_API int pac_memcpy_d2h(void* dst, const void* src, size_t bytes, pac_stream_t stream);
+PAC_API int pac_memcpy_d2d(void* dst, const void* src, size_t bytes, pac_stream_t stream);
+PAC_API int pac_stream_create(pac_stream_t* stream);
+PAC_API int pac_stream_destroy(pac_stream_t stream);
+PAC_API int pac_stream_synchronize(pac_stream_t stream);
+/* Work queued on `waiter` after this call starts when the work queued so far
+ * on `waitee` has finished (an event recorded on waitee). */
+PAC_API int pac_stream_wait_stream(pac_stream_t waiter, pac_stream_t waitee);
+
+/* Number of this library's kernel launches since load (for accounting). */
+PAC_API long long pac_launch_count(void);
+
+PAC_API const char* pac_status_string(int status);
+/* Message of the last failed call on this host thread ("" if none). */
+PAC_API const char* pac_last_error(void);
+/* Status of the last failed fft.h drop-in call on this thread, then clears it
+ * (the fft.h entry points return void, as in the reference). */
+PAC_API int pac_get_last_status(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PAC_H */
