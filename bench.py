@@ -1,0 +1,526 @@
+#!/usr/bin/env python
+"""Benchmark of the permutation-avoiding FFT convolution on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--config c3|c1|c2|c4|c4a] [--form f64|f32]
+
+A step is one convolution of one batch of the configuration's synthetic
+input.  The default workload is C3: a 2D 2048 x 2048 complex FP64 circular
+convolution with a 31 x 31 Gaussian filter (the configuration the north-star
+target is quoted on).  ``value`` times K steps of pac_convolve on
+device-resident data (CUDA events, inputs larger than L2, max over ranks);
+``e2e`` times the reference-compatible call
+permutation_avoiding_convolution_2d on pinned host buffers, copies included.
+
+--impl reference times the reference's own CPU code (oracle/_ref, compiled
+from the reference sources) on the host cores, one process per core.
+
+Multi-GPU (torchrun): replicas -- every rank convolves its own batch, no
+collective on the data path; value = all ranks' elements / max-over-ranks time.
+"""
+import argparse
+import importlib
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+PKG = "c-permutation-avoiding-convolution_b200"
+pac = importlib.import_module(PKG)
+W = importlib.import_module(PKG + ".workloads")
+
+METRIC = "conv GElem/s & % HBM roofline; FP32/TC vs FP64 GPU at <=1e-6 rel L2"
+
+CONFIGS = {
+    "c3": dict(dims=(2048, 2048), batch=1, radix=2,
+               workload="2D 2048x2048 complex circular convolution, real 31x31 Gaussian "
+                        "filter (sigma 5) zero-padded and centred, x ~ U(-1,1)"),
+    "c1": dict(dims=(4096,), batch=1, radix=4,
+               workload="1D n=2^12 complex circular convolution, radix-4 digit order, "
+                        "x, h ~ N(0,1)"),
+    "c2": dict(dims=(65536,), batch=1024, radix=4,
+               workload="1D batch 1024 x n=2^16 complex circular convolution, one 257-tap "
+                        "N(0,1/257) filter"),
+    "c4": dict(dims=(256, 256, 256), batch=1, radix=2,
+               workload="3D 256^3 complex circular convolution, 9x9x9 N(0,1/729) stencil"),
+    "c4a": dict(dims=(512, 256, 128), batch=1, radix=2,
+                workload="3D 512x256x128 complex circular convolution, 9x9x9 N(0,1/729) "
+                         "stencil"),
+}
+
+# DRAM bytes per convolution (sum over its passes) from one ncu capture of
+# the same command; the capture, its command line and the per-kernel figures
+# are in profiles/.
+MEASURED_TRAFFIC = {}
+
+
+def make_inputs(cfg_name, batch=None):
+    if cfg_name == "c3":
+        return W.c3()
+    if cfg_name == "c1":
+        return W.c1()
+    if cfg_name == "c2":
+        return W.c2(batch=batch or 1024)
+    if cfg_name == "c4":
+        return W.c4((256, 256, 256))
+    if cfg_name == "c4a":
+        return W.c4((512, 256, 128))
+    raise ValueError(cfg_name)
+
+
+def read_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# CPU side: the reference's own code (or the oracle port) on the host cores
+# ---------------------------------------------------------------------------
+def _cpu_lib():
+    ref = os.path.join(ROOT, "oracle", "_ref", "libref_fast.so")
+    if os.path.exists(ref):
+        return ref, "reference"
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    return O.build_orc(), "port"
+
+
+_CPU = {}
+
+
+def _cpu_init(cfg_name, libpath, kind):
+    """Per host process: load the CPU library and build the inputs once."""
+    import ctypes as C
+    cfg = CONFIGS[cfg_name]
+    dims, r = cfg["dims"], cfg["radix"]
+    x, h = make_inputs(cfg_name, batch=1)
+    x = x.reshape(dims)
+    L = C.CDLL(libpath)
+    dp = C.POINTER(C.c_double)
+    x0 = (np.ascontiguousarray(x.real), np.ascontiguousarray(x.imag))
+    h0 = (np.ascontiguousarray(h.real.reshape(dims)), np.ascontiguousarray(h.imag.reshape(dims)))
+    xr, xi = x0[0].copy(), x0[1].copy()
+    hr, hi = h0[0].copy(), h0[1].copy()
+    nd = len(dims)
+    if kind == "reference":
+        tw = []
+        for n in dims:
+            pr, pi = C.POINTER(dp)(), C.POINTER(dp)()
+            getattr(L, f"precompute_twiddles_r{r}")(n, C.byref(pr), C.byref(pi))
+            tw += [pr, pi]
+        f = getattr(L, "permutation_avoiding_convolution" + ("" if nd == 1 else f"_{nd}d"))
+
+        def call():
+            f(xr.ctypes.data_as(dp), xi.ctypes.data_as(dp), *[C.c_int(v) for v in dims],
+              C.c_int(r), *tw, hr.ctypes.data_as(dp), hi.ctypes.data_as(dp))
+    else:
+        arr = (C.c_int * nd)(*dims)
+        L.orc_convolution_nd.argtypes = [C.c_int, C.c_int, dp, dp, C.c_int, C.POINTER(C.c_int),
+                                         dp, dp]
+
+        def call():
+            L.orc_convolution_nd(1, r, xr.ctypes.data_as(dp), xi.ctypes.data_as(dp), nd, arr,
+                                 hr.ctypes.data_as(dp), hi.ctypes.data_as(dp))
+    _CPU.update(call=call, h=(hr, hi), h0=h0)
+
+
+def _cpu_task(args):
+    """Time reference convolutions until `seconds` of busy time (at least
+    min_count calls).  Returns (convolutions, busy seconds)."""
+    seconds, min_count = args
+    hr, hi = _CPU["h"]
+    count, busy = 0, 0.0
+    while count < min_count or busy < seconds:
+        np.copyto(hr, _CPU["h0"][0])  # the call overwrites h with A^T h; restored
+        np.copyto(hi, _CPU["h0"][1])  # outside the timing, as the reference's drivers do
+        t0 = time.perf_counter()
+        _CPU["call"]()
+        busy += time.perf_counter() - t0
+        count += 1
+    return count, busy
+
+
+class CpuPool:
+    """`procs` spawned host processes running the reference's convolution on
+    the configuration's input (one problem of the batch per call)."""
+
+    def __init__(self, cfg_name, procs):
+        self.libpath, self.kind = _cpu_lib()
+        self.procs = procs
+        self.n_el = int(np.prod(CONFIGS[cfg_name]["dims"]))
+        self.pool = mp.get_context("spawn").Pool(
+            procs, initializer=_cpu_init, initargs=(cfg_name, self.libpath, self.kind))
+
+    def rate(self, seconds, min_count=1):
+        """GElem/s summed over the processes, each over its own busy time."""
+        res = self.pool.map(_cpu_task, [(seconds, min_count)] * self.procs, chunksize=1)
+        convs = sum(c for c, _ in res)
+        return sum(c * self.n_el / b for c, b in res) / 1e9, convs, sum(b for _, b in res)
+
+    def close(self):
+        self.pool.close()
+        self.pool.join()
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region (nvidia-smi in a separate process)
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = os.path.join("/tmp", f"pac_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "50"],
+                stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        rows = []
+        for line in open(self.path):
+            p = [v.strip() for v in line.split(",")]
+            if len(p) >= 9:
+                rows.append(p)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+
+        def num(v):
+            try:
+                return float(v)
+            except ValueError:
+                return None
+        sm = [num(r[1]) for r in rows if num(r[1]) is not None]
+        mx = [num(r[2]) for r in rows if num(r[2]) is not None]
+        pw = [num(r[3]) for r in rows if num(r[3]) is not None]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows), "power_w_max": max(pw) if pw else None}
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def pass_names(n):
+    m = (n + 1) // 2
+    names = [f"DIF factor {i}" for i in range(m - 1)] + ["fused innermost: DIF, x Hhat, DIT"]
+    names += [f"DIT factor {i}" for i in range(m - 2, -1, -1)]
+    return names
+
+
+def run_ours(args, world, dist):
+    import ctypes as C
+
+    import torch
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    cfg = CONFIGS[args.config]
+    dims, batch = cfg["dims"], cfg["batch"]
+    N = int(np.prod(dims))
+    form = pac.PAC_FORM_F64 if args.form == "f64" else pac.PAC_FORM_F32
+    tdt = torch.float64 if form == pac.PAC_FORM_F64 else torch.float32
+    esz = 8 if form == pac.PAC_FORM_F64 else 4
+    L = pac.load()
+    x, h = make_inputs(args.config)
+    x = x.reshape((batch,) + dims)
+    h = h.reshape(dims)
+
+    def t(a):
+        return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+
+    # device inputs: x rotated over R buffers so that no step reads an
+    # L2-resident input (L2 is 126 MB)
+    per = batch * N * esz * 2
+    R = 2 if per >= 384e6 else min(8, int(np.ceil(384e6 / per)) + 1)
+    xs = [(t(x.real).to(tdt), t(x.imag).to(tdt)) for _ in range(R)]
+    hd = (t(h.real), t(h.imag))
+    Hh = (torch.empty(dims, dtype=tdt, device=dev), torch.empty(dims, dtype=tdt, device=dev))
+    y = (torch.empty((batch,) + dims, dtype=tdt, device=dev),
+         torch.empty((batch,) + dims, dtype=tdt, device=dev))
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+    plan = pac.Plan(L, dims, batch, 2, form)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    plan.filter_spectrum(hd[0].data_ptr(), hd[1].data_ptr(), Hh[0].data_ptr(), Hh[1].data_ptr(),
+                         stream=sp)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    spectrum_ms = ev0.elapsed_time(ev1)
+
+    def step(k):
+        a = xs[k % R]
+        plan.convolve(a[0].data_ptr(), a[1].data_ptr(), Hh[0].data_ptr(), Hh[1].data_ptr(),
+                      y[0].data_ptr(), y[1].data_ptr(), stream=sp)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    for k in range(args.warmup):
+        step(k)
+    barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    launches0 = L.pac_launch_count()
+    t_wall = time.perf_counter()
+    ev0.record(stream)
+    for k in range(args.steps):
+        step(k)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    launches = L.pac_launch_count() - launches0
+    barrier()
+    ms = ev0.elapsed_time(ev1)
+    # the same load continues (untimed) until ~1.5 s have passed so that the
+    # 50 ms clock sampler sees the steps' clocks even for short timed regions
+    k = 0
+    while time.perf_counter() - t_wall < 1.5:
+        for _ in range(20):
+            step(k)
+            k += 1
+        torch.cuda.synchronize()
+    clocks = sampler.stop()
+    if dist is not None:
+        tt = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    ms_step = ms / args.steps
+    value = world * batch * N / (ms_step * 1e-3) / 1e9
+
+    # per-pass durations: the same steps with CUDA events around every pass
+    pac.check(L, L.pac_plan_set_pass_timing(plan.h, 1), "timing")
+    for k in range(min(args.steps, 200)):
+        step(k)
+    buf = (C.c_double * 16)()
+    calls, npass = C.c_longlong(), C.c_int()
+    L.pac_plan_get_pass_timing(plan.h, 16, buf, C.byref(calls), C.byref(npass))
+    pac.check(L, L.pac_plan_set_pass_timing(plan.h, 0), "timing")
+    pass_ms = [buf[i] / max(calls.value, 1) for i in range(npass.value)]
+
+    # the result of this run against numpy's FP64 FFT
+    step(0)
+    torch.cuda.synchronize()
+    rows = [0] if batch == 1 else [0, batch - 1]
+    errs = []
+    axes = tuple(range(len(dims)))
+    Hf = np.fft.fftn(h)
+    for b in rows:
+        got = y[0][b].double().cpu().numpy() + 1j * y[1][b].double().cpu().numpy()
+        want = np.fft.ifftn(np.fft.fftn(x[b], axes=axes) * Hf, axes=axes)
+        errs.append(float(np.linalg.norm((got - want).ravel()) / np.linalg.norm(want.ravel())))
+
+    peak, peak_kind = read_peaks()
+    alg_bytes = 3 * batch * N * 2 * esz  # read x + read Hhat + write y
+    achieved = alg_bytes / (ms_step * 1e-3) / 1e9
+    tot = sum(pass_ms) or 1.0
+    passes = []
+    for nm, pm in zip(pass_names(len(pass_ms)), pass_ms):
+        mb = (3 if nm.startswith("fused") else 2) * batch * N * 2 * esz
+        passes.append({"pass": nm, "ms": round(pm, 5), "share": round(pm / tot, 3),
+                       "min_bytes": mb, "GB/s": round(mb / (pm * 1e-3) / 1e9, 1)})
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4),
+                "traffic": MEASURED_TRAFFIC.get((args.config, args.form)),
+                "peak_source": "measured, MEASURED_PEAKS.json hbm_gbs" if peak_kind == "measured"
+                else "fallback 6650 GB/s",
+                "kernel": f"pac_pass_kernel x{len(pass_ms)} = one convolution",
+                "algorithmic_bytes_per_step": alg_bytes, "passes": passes}
+    out = {"metric": METRIC, "value": round(value, 3), "unit": "GElem/s", "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 5),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": args.form,
+           "data": "synthetic, seeded (numpy default_rng); the reference uses no dataset",
+           "config": {"workload": cfg["workload"], "dims": list(dims), "batch": batch,
+                      "form": args.form, "digit_base": 2, "passes": len(pass_ms),
+                      "l2": f"inputs larger than L2: x rotated over {R} buffers of "
+                            f"{per / 2**20:.0f} MiB; Hhat {N * esz * 2 / 2**20:.0f} MiB",
+                      "parallelism": f"replicas x{world}"},
+           "roofline": roofline, "gpu_launches": int(launches), "clocks": clocks,
+           "filter_spectrum_ms": round(spectrum_ms, 4), "rel_l2_vs_numpy_fp64": max(errs)}
+    plan.close()
+    return out
+
+
+def run_e2e(args, world, dist):
+    """The reference-facing call on pinned host buffers: H2D, transforms, D2H."""
+    import ctypes as C
+
+    import torch
+
+    cfg = CONFIGS[args.config]
+    dims = cfg["dims"]
+    N = int(np.prod(dims))
+    L = pac.load()
+    x, h = make_inputs(args.config, batch=1)
+    x = x.reshape((-1,) + dims)[0]
+    h = h.reshape(dims)
+    arrs = [torch.empty(dims, dtype=torch.float64, pin_memory=True).numpy() for _ in range(4)]
+    dp = C.POINTER(C.c_double)
+    nd = len(dims)
+    name = "permutation_avoiding_convolution" + ("" if nd == 1 else f"_{nd}d")
+    f = getattr(L, name)
+    r = cfg["radix"]
+    steps = max(3, min(args.steps, 20))
+    times = []
+    for k in range(2 + steps):
+        np.copyto(arrs[0], x.real)
+        np.copyto(arrs[1], x.imag)
+        np.copyto(arrs[2], h.real)  # the call overwrites h with A^T h
+        np.copyto(arrs[3], h.imag)
+        t0 = time.perf_counter()
+        f(arrs[0].ctypes.data_as(dp), arrs[1].ctypes.data_as(dp), *[int(v) for v in dims], r,
+          *([None] * (2 * nd)), arrs[2].ctypes.data_as(dp), arrs[3].ctypes.data_as(dp))
+        dt = time.perf_counter() - t0
+        if L.pac_get_last_status():
+            raise RuntimeError(L.pac_last_error().decode())
+        if k >= 2:
+            times.append(dt)
+    tm = sum(times) / len(times)
+    if dist is not None:
+        tt = torch.tensor([tm], device=torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0))),
+                          dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        tm = float(tt.item())
+    return {"value": round(world * N / tm / 1e9, 4), "unit": "GElem/s",
+            "h2d_bytes_per_step": 4 * N * 8, "d2h_bytes_per_step": 4 * N * 8,
+            "call": f"{name} (fft.h, radix {r}) on pinned host buffers, mean of {steps} calls",
+            "ms_per_call": round(tm * 1e3, 3)}
+
+
+def run_reference(args):
+    cfg = CONFIGS[args.config]
+    procs = max(1, min(os.cpu_count() or 1, 64))
+    n_el = int(np.prod(cfg["dims"]))
+    one = CpuPool(args.config, 1)
+    r1, _, _ = one.rate(0.0, 1)
+    one.close()
+    per_conv = n_el / (r1 * 1e9)
+    pool = CpuPool(args.config, procs)
+    per_step = max(per_conv, 0.25)  # one step: every core busy for >= 0.25 s
+    k_run = max(1, min(args.steps, int(150.0 / per_step)))
+    for _ in range(min(args.warmup, 2)):
+        pool.rate(0.0, 1)
+    t0 = time.perf_counter()
+    rates, convs = [], 0
+    for _ in range(k_run):
+        rate, c, _ = pool.rate(per_step, 1)
+        rates.append(rate)
+        convs += c
+    wall = time.perf_counter() - t0
+    pool.close()
+    value = statistics.mean(rates)
+    desc = {"value": round(value, 6), "unit": "GElem/s", "cores": procs, "kind": pool.kind,
+            "sample": f"{k_run} steps (of {args.steps} requested), each {procs} processes x "
+                      f">= {per_step:.2f} s of convolutions ({convs} in all, "
+                      f"{per_conv * 1e3:.2f} ms per convolution on one core), "
+                      f"permutation_avoiding_convolution from "
+                      f"{os.path.relpath(pool.libpath, ROOT)}"}
+    return {"metric": METRIC, "value": round(value, 6), "unit": "GElem/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(wall / k_run * 1e3, 2), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic, seeded (numpy default_rng)",
+            "config": {"workload": cfg["workload"], "dims": list(cfg["dims"]),
+                       "batch": cfg["batch"], "form": "f64", "parallelism": "host cores"},
+            "impl": "reference", "cpu_baseline": desc,
+            "e2e": {"value": round(value, 6), "unit": "GElem/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", choices=sorted(CONFIGS), default="c3")
+    ap.add_argument("--form", choices=["f64", "f32"], default="f64")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--no-forms", action="store_true", help="skip the FP32 comparison")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)), flush=True)
+        return 0
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = tdist
+    out = run_ours(args, world, dist)
+    out["e2e"] = run_e2e(args, world, dist)
+    if not args.no_forms and args.form == "f64":
+        a32 = argparse.Namespace(**vars(args))
+        a32.form = "f32"
+        o32 = run_ours(a32, world, dist)
+        out["forms"] = {
+            "f64": {"value": out["value"], "rel_l2_vs_numpy_fp64": out["rel_l2_vs_numpy_fp64"],
+                    "roofline_frac": out["roofline"]["frac"]},
+            "f32": {"value": o32["value"], "rel_l2_vs_numpy_fp64": o32["rel_l2_vs_numpy_fp64"],
+                    "speedup_vs_f64": round(o32["value"] / out["value"], 3),
+                    "roofline_frac": o32["roofline"]["frac"],
+                    "passes": o32["roofline"]["passes"]}}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        procs = min(os.cpu_count() or 1, 16)
+        pool = CpuPool(args.config, procs)
+        rate, convs, busy = pool.rate(1.5, 1)
+        pool.close()
+        out["cpu_baseline"] = {
+            "value": round(rate, 6), "unit": "GElem/s", "cores": procs, "kind": pool.kind,
+            "sample": f"{convs} convolutions of the workload on {procs} processes (>= 1.5 s "
+                      f"each, {busy:.1f} s of CPU work), "
+                      f"{os.path.relpath(pool.libpath, ROOT)}"}
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

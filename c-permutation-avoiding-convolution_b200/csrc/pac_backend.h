@@ -23,6 +23,11 @@ int be_stream_create(void** s);
 int be_stream_destroy(void* s);
 int be_stream_sync(void* s);
 int be_stream_wait(void* waiter, void* waitee);
+// timing events: record on a stream, elapsed milliseconds between two
+int be_event_create(void** ev);
+int be_event_destroy(void* ev);
+int be_event_record(void* ev, void* stream);
+int be_event_elapsed(void* a, void* b, float* ms);  // waits for b
 
 // one pass over `grid` CTAs (elem_bytes 8: double, 4: float; b2 = log2 base)
 int be_launch_pass(const PassDesc& d, int elem_bytes, int b2, long long grid, int threads,

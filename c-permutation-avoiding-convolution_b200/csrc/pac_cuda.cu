@@ -235,6 +235,25 @@ int be_stream_sync(void* s) {
   PAC_CU(cudaStreamSynchronize((cudaStream_t)s), "cudaStreamSynchronize");
   return PAC_SUCCESS;
 }
+int be_event_create(void** ev) {
+  cudaEvent_t e;
+  PAC_CU(cudaEventCreate(&e), "cudaEventCreate");
+  *ev = e;
+  return PAC_SUCCESS;
+}
+int be_event_destroy(void* ev) {
+  if (ev) cudaEventDestroy((cudaEvent_t)ev);
+  return PAC_SUCCESS;
+}
+int be_event_record(void* ev, void* stream) {
+  PAC_CU(cudaEventRecord((cudaEvent_t)ev, (cudaStream_t)stream), "cudaEventRecord");
+  return PAC_SUCCESS;
+}
+int be_event_elapsed(void* a, void* b, float* ms) {
+  PAC_CU(cudaEventSynchronize((cudaEvent_t)b), "cudaEventSynchronize");
+  PAC_CU(cudaEventElapsedTime(ms, (cudaEvent_t)a, (cudaEvent_t)b), "cudaEventElapsedTime");
+  return PAC_SUCCESS;
+}
 int be_stream_wait(void* waiter, void* waitee) {
   cudaEvent_t ev;
   PAC_CU(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "cudaEventCreate");

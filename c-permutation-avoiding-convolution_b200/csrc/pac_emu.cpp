@@ -48,6 +48,16 @@ int be_stream_create(void** s) {
 int be_stream_destroy(void*) { return PAC_SUCCESS; }
 int be_stream_sync(void*) { return PAC_SUCCESS; }
 int be_stream_wait(void*, void*) { return PAC_SUCCESS; }
+int be_event_create(void** ev) {
+  *ev = nullptr;
+  return PAC_SUCCESS;
+}
+int be_event_destroy(void*) { return PAC_SUCCESS; }
+int be_event_record(void*, void*) { return PAC_SUCCESS; }
+int be_event_elapsed(void*, void*, float* ms) {
+  *ms = 0.f;
+  return PAC_SUCCESS;
+}
 
 template <typename T, int B2>
 static void replay(const PassDesc& d, long long grid) {

@@ -27,6 +27,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -205,9 +206,16 @@ struct pac_plan_s {
   size_t ws_bytes = 0;
   void* tmp64 = nullptr;  // FP64 temporary for the F32 filter spectrum
   size_t tmp64_bytes = 0;
+  // per-pass timing (pac_plan_set_pass_timing)
+  int timing = 0;
+  std::mutex t_mu;
+  std::vector<void*> t_ev;
+  std::vector<double> t_ms;
+  long long t_calls = 0;
   ~pac_plan_s() {
     if (ws) pac::be_free(ws);
     if (tmp64) pac::be_free(tmp64);
+    for (void* e : t_ev) pac::be_event_destroy(e);
   }
 };
 
@@ -298,6 +306,39 @@ static int launch(const Schedule& s, PassSpec& p, void* stream) {
   return be_launch_pass(p.d, s.bytes, s.b2, p.grid, p.threads, p.smem, stream);
 }
 
+// Launch a pass list; with pass timing enabled, bracket every pass with
+// events and accumulate the per-pass milliseconds in the plan.
+static int exec_passes(pac_plan_s* pl, const Schedule& s, std::vector<PassSpec>& passes,
+                       void* stream) {
+  if (!pl->timing) {
+    for (auto& p : passes) PAC_TRY(launch(s, p, stream));
+    return PAC_SUCCESS;
+  }
+  std::lock_guard<std::mutex> g(pl->t_mu);
+  const size_t n = passes.size();
+  while (pl->t_ev.size() < n + 1) {
+    void* ev = nullptr;
+    PAC_TRY(be_event_create(&ev));
+    pl->t_ev.push_back(ev);
+  }
+  if (pl->t_ms.size() != n) {
+    pl->t_ms.assign(n, 0.0);
+    pl->t_calls = 0;
+  }
+  PAC_TRY(be_event_record(pl->t_ev[0], stream));
+  for (size_t i = 0; i < n; ++i) {
+    PAC_TRY(launch(s, passes[i], stream));
+    PAC_TRY(be_event_record(pl->t_ev[i + 1], stream));
+  }
+  for (size_t i = 0; i < n; ++i) {
+    float ms = 0.f;
+    PAC_TRY(be_event_elapsed(pl->t_ev[i], pl->t_ev[i + 1], &ms));
+    pl->t_ms[i] += ms;
+  }
+  pl->t_calls++;
+  return PAC_SUCCESS;
+}
+
 static int get_ws(pac_plan_s* pl, size_t bytes, void** out) {
   if (pl->ws_bytes < bytes) {
     if (pl->ws) be_free(pl->ws);
@@ -383,11 +424,11 @@ static int run_transform(pac_plan_s* pl, const Schedule& s, int op, long long ba
     p.d.in_im = src_im;
     p.d.out_re = bre[dst];
     p.d.out_im = bim[dst];
-    PAC_TRY(launch(s, p, stream));
     cur = dst;
     src_re = bre[cur];
     src_im = bim[cur];
   }
+  PAC_TRY(exec_passes(pl, s, passes, stream));
   if (cur != 0) PAC_TRY(be_memcpy(out_re, bre[cur], arr_bytes, CPY_D2D, stream));
   if (cur != 0) PAC_TRY(be_memcpy(out_im, bim[cur], arr_bytes, CPY_D2D, stream));
   return PAC_SUCCESS;
@@ -403,6 +444,7 @@ static int run_conv(pac_plan_s* pl, const void* x_re, const void* x_im, const vo
   if (m == 0)
     return be_pointwise(pl->batch * N, s.bytes, x_re, x_im, h_re, h_im, hmask, y_re, y_im, scale,
                         stream);
+  std::vector<PassSpec> passes;
   for (int vi = 0; vi < m - 1; ++vi) {
     PassSpec p = make_pass(s, vi, pl->batch, N);
     p.d.mode = MODE_DIF;
@@ -412,7 +454,7 @@ static int run_conv(pac_plan_s* pl, const void* x_re, const void* x_im, const vo
     p.d.in_im = vi == 0 ? x_im : y_im;
     p.d.out_re = y_re;
     p.d.out_im = y_im;
-    PAC_TRY(launch(s, p, stream));
+    passes.push_back(p);
   }
   {
     PassSpec p = make_pass(s, m - 1, pl->batch, N);
@@ -425,7 +467,7 @@ static int run_conv(pac_plan_s* pl, const void* x_re, const void* x_im, const vo
     p.d.in_im = m == 1 ? x_im : y_im;
     p.d.out_re = y_re;
     p.d.out_im = y_im;
-    PAC_TRY(launch(s, p, stream));
+    passes.push_back(p);
   }
   for (int vi = m - 2; vi >= 0; --vi) {
     PassSpec p = make_pass(s, vi, pl->batch, N);
@@ -436,9 +478,9 @@ static int run_conv(pac_plan_s* pl, const void* x_re, const void* x_im, const vo
     p.d.in_im = y_im;
     p.d.out_re = y_re;
     p.d.out_im = y_im;
-    PAC_TRY(launch(s, p, stream));
+    passes.push_back(p);
   }
-  return PAC_SUCCESS;
+  return exec_passes(pl, s, passes, stream);
 }
 
 }  // namespace pac
@@ -643,6 +685,29 @@ PAC_API int pac_stream_wait_stream(pac_stream_t waiter, pac_stream_t waitee) {
   return be_stream_wait(waiter, waitee);
 }
 PAC_API long long pac_launch_count(void) { return be_launch_count(); }
+
+PAC_API int pac_plan_set_pass_timing(pac_plan_t plan, int enable) {
+  if (!plan) return set_error(PAC_ERROR_INVALID_VALUE, "pac_plan_set_pass_timing: NULL");
+  std::lock_guard<std::mutex> g(plan->t_mu);
+  plan->timing = enable ? 1 : 0;
+  plan->t_ms.clear();
+  plan->t_calls = 0;
+  return PAC_SUCCESS;
+}
+
+PAC_API int pac_plan_get_pass_timing(pac_plan_t plan, int max_passes, double* ms, long long* calls,
+                                     int* npasses) {
+  if (!plan || !npasses) return set_error(PAC_ERROR_INVALID_VALUE, "pac_plan_get_pass_timing: NULL");
+  std::lock_guard<std::mutex> g(plan->t_mu);
+  *npasses = (int)plan->t_ms.size();
+  for (int i = 0; i < *npasses && i < max_passes; ++i) {
+    if (ms) ms[i] = plan->t_ms[i];
+  }
+  if (calls) *calls = plan->t_calls;
+  std::fill(plan->t_ms.begin(), plan->t_ms.end(), 0.0);
+  plan->t_calls = 0;
+  return PAC_SUCCESS;
+}
 
 PAC_API const char* pac_status_string(int status) {
   switch (status) {

@@ -163,6 +163,15 @@ PAC_API int pac_stream_synchronize(pac_stream_t stream);
  * on `waitee` has finished (an event recorded on waitee). */
 PAC_API int pac_stream_wait_stream(pac_stream_t waiter, pac_stream_t waitee);
 
+/* Per-pass timing: while enabled, pac_convolve and pac_transform record a
+ * CUDA event before the first and after every pass on the caller's stream
+ * and wait for them at the end of the call (so calls become synchronous).
+ * pac_plan_get_pass_timing returns, per pass slot of the last operator, the
+ * summed milliseconds and the number of timed calls, then resets them. */
+PAC_API int pac_plan_set_pass_timing(pac_plan_t plan, int enable);
+PAC_API int pac_plan_get_pass_timing(pac_plan_t plan, int max_passes, double* ms,
+                                     long long* calls, int* npasses);
+
 /* Number of this library's kernel launches since load (for accounting). */
 PAC_API long long pac_launch_count(void);
 

@@ -252,11 +252,13 @@ void orc_rho(int r, int rank, const int* dims, int* rho) {
   }
 }
 
-/* swap-based in-place permutation (index_reversals.c:85-94) */
+/* swap-based in-place permutation (index_reversals.c:85-94).  Indices past
+ * the array (a digit reversal built for a length that is not a power of r)
+ * are skipped instead of written out of bounds. */
 void orc_apply_permutation_split(double* re, double* im, long n, const int* rho) {
   for (long j = 0; j < n; ++j) {
     long p = rho[j];
-    if (j < p) {
+    if (j < p && p < n) {
       double a = re[j], b = im[j];
       re[j] = re[p];
       im[j] = im[p];

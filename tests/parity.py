@@ -1,0 +1,138 @@
+"""Parity checks shared by the host-replay tests (test_emulated.py, CPU) and
+the GPU tests (test_gpu_*.py).  Each check calls the library through its C
+ABI and compares with the oracle."""
+import ctypes as C
+
+import numpy as np
+
+from conftest import O, pac, rel_l2, rng
+
+TOL = 1e-13  # FP64 forms vs the FP64 oracle (north star: 1e-13 relative L2)
+TOL_F32 = 1e-6  # FP32 form vs the FP64 oracle
+
+OPS = ((O.OP_A, "A"), (O.OP_CONJ, "conjA"), (O.OP_AT, "At"))
+KINDS = ("fft", "fft2", "ufft", "ifft", "uifft")
+
+
+def check_golden(L, g):
+    """Every drop-in entry point against the reference's own outputs."""
+    r = int(g["r"])
+    x = (g["x_re"], g["x_im"])
+    h = (g["h_re"], g["h_im"])
+    errs = {}
+    if "At_re" in g:
+        for op, name in OPS:
+            a = pac.dropin_butterflies(L, op, r, *x)
+            errs[name] = rel_l2(*a, g[name + "_re"], g[name + "_im"])
+        for k, name in enumerate(KINDS):
+            a = pac.dropin_transform(L, k, r, *x, rho=g["rho"])
+            errs[name] = rel_l2(*a, g[name + "_re"], g[name + "_im"])
+        y = pac.dropin_convolution(L, O.METHOD_FFT_BASED, r, *x, *h, rho=g["rho"])
+        errs["fbc"] = rel_l2(y[0], y[1], g["fbc_re"], g["fbc_im"])
+        errs["fbc_h"] = rel_l2(y[2], y[3], g["fbc_hre"], g["fbc_him"])
+    y = pac.dropin_convolution(L, O.METHOD_PAC, r, *x, *h)
+    errs["pac"] = rel_l2(y[0], y[1], g["pac_re"], g["pac_im"])
+    errs["pac_h"] = rel_l2(y[2], y[3], g["pac_hre"], g["pac_him"])
+    bad = {k: v for k, v in errs.items() if not v < TOL}
+    assert not bad, bad
+
+
+def check_against_oracle(L, orc, shape, r, seed=0, ops=True):
+    g = rng(seed)
+    x = (g.standard_normal(shape), g.standard_normal(shape))
+    h = (g.standard_normal(shape), g.standard_normal(shape))
+    errs = {}
+    if ops:
+        for op, name in OPS:
+            errs[name] = rel_l2(*pac.dropin_butterflies(L, op, r, *x), *orc.butterflies(op, r, *x))
+        rho = orc.rho(r, shape)
+        for k, name in enumerate(KINDS):
+            errs[name] = rel_l2(*pac.dropin_transform(L, k, r, *x, rho=rho),
+                                *orc.transform(k, r, *x))
+    y = pac.dropin_convolution(L, O.METHOD_PAC, r, *x, *h)
+    z = orc.convolution(O.METHOD_PAC, r, *x, *h)
+    errs["pac"] = rel_l2(y[0], y[1], z[0], z[1])
+    # the overwritten filter is A^T h in P_r order: the index maps must agree
+    errs["pac_h"] = rel_l2(y[2], y[3], z[2], z[3])
+    bad = {k: v for k, v in errs.items() if not v < TOL}
+    assert not bad, bad
+
+
+class Dev:
+    """Device buffers through the library's own pac_malloc (host memory in
+    the emulator build, device memory in the product)."""
+
+    def __init__(self, L):
+        self.L = L
+        self.ptrs = []
+
+    def put(self, a):
+        a = np.ascontiguousarray(a)
+        p = C.c_void_p()
+        pac.check(self.L, self.L.pac_malloc(C.byref(p), max(a.nbytes, 16)), "pac_malloc")
+        self.ptrs.append(p)
+        pac.check(self.L, self.L.pac_memcpy_h2d(p, a.ctypes.data, a.nbytes, None), "h2d")
+        return p
+
+    def zeros(self, shape, dtype):
+        return self.put(np.zeros(shape, dtype))
+
+    def get(self, p, shape, dtype):
+        out = np.empty(shape, dtype)
+        pac.check(self.L, self.L.pac_memcpy_d2h(out.ctypes.data, p, out.nbytes, None), "d2h")
+        pac.check(self.L, self.L.pac_stream_synchronize(None), "sync")
+        return out
+
+    def free(self):
+        for p in self.ptrs:
+            self.L.pac_free(p)
+        self.ptrs = []
+
+
+def native_conv(L, dims, batch, base, form, x, h, per_problem=False):
+    """pac_filter_spectrum + pac_convolve on host arrays; returns y (complex)."""
+    dt = np.float64 if form == pac.PAC_FORM_F64 else np.float32
+    d = Dev(L)
+    try:
+        plan = pac.Plan(L, dims, batch, base, form)
+        nf = batch if per_problem else 1
+        hshape = (nf,) + tuple(dims)
+        hr = d.put(np.real(h).reshape(hshape).astype(np.float64))
+        hi = d.put(np.imag(h).reshape(hshape).astype(np.float64))
+        Hr, Hi = d.zeros(hshape, dt), d.zeros(hshape, dt)
+        plan.filter_spectrum(hr, hi, Hr, Hi, nfilters=nf)
+        shape = (batch,) + tuple(dims)
+        xr = d.put(np.real(x).reshape(shape).astype(dt))
+        xi = d.put(np.imag(x).reshape(shape).astype(dt))
+        yr, yi = d.zeros(shape, dt), d.zeros(shape, dt)
+        plan.convolve(xr, xi, Hr, Hi, yr, yi, per_problem=1 if per_problem else 0)
+        y = d.get(yr, shape, dt) + 1j * d.get(yi, shape, dt)
+        plan.close()
+        return y
+    finally:
+        d.free()
+
+
+def native_transform(L, dims, batch, base, form, op, x):
+    dt = np.float64 if form == pac.PAC_FORM_F64 else np.float32
+    d = Dev(L)
+    try:
+        plan = pac.Plan(L, dims, batch, base, form)
+        shape = (batch,) + tuple(dims)
+        xr = d.put(np.real(x).reshape(shape).astype(dt))
+        xi = d.put(np.imag(x).reshape(shape).astype(dt))
+        yr, yi = d.zeros(shape, dt), d.zeros(shape, dt)
+        plan.transform(op, xr, xi, yr, yi)
+        y = d.get(yr, shape, dt) + 1j * d.get(yi, shape, dt)
+        plan.close()
+        return y
+    finally:
+        d.free()
+
+
+def fftconv(x, h, axes):
+    return np.fft.ifftn(np.fft.fftn(x, axes=axes) * np.fft.fftn(h, axes=axes), axes=axes)
+
+
+def crel(a, b):
+    return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))

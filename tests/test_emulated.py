@@ -1,0 +1,148 @@
+"""Host replay of the device passes (TEST-ONLY libpac_emu.so) against the
+oracle: the plan layer, the pass geometry, the digit-reversal index maps and
+the 4-step twiddles, checked on the CPU with the same code the sm_100a
+kernel runs.  The GPU versions of these checks are in test_gpu_parity.py."""
+import os
+
+import numpy as np
+import pytest
+
+import parity as P
+from conftest import O, pac, rel_l2, rng
+
+
+def test_golden(emu, golden):
+    P.check_golden(emu, golden)
+
+
+@pytest.mark.parametrize("shape,r", [((8192,), 2), ((4 ** 7,), 4), ((8 ** 5,), 8),
+                                     ((8192, 4), 2), ((4, 8192), 2), ((16, 64, 16), 4),
+                                     ((128, 4, 4), 2), ((1,), 2), ((2,), 2), ((1,), 8)])
+def test_oracle_sizes(emu, orc, shape, r):
+    P.check_against_oracle(emu, orc, shape, r, ops=np.prod(shape) <= 2 ** 15)
+
+
+@pytest.mark.parametrize("cap", ["3", "4", "6"])
+def test_multi_factor_splits(emu, orc, cap, monkeypatch):
+    """Force 2-4 factors per axis (4-step twiddles between every pair, the
+    natural-order store across factors)."""
+    monkeypatch.setenv("PAC_MAX_FACTOR_LOG", cap)
+    for shape, r in [((2 ** 12,), 2), ((4 ** 6,), 4), ((8 ** 4,), 8), ((128, 32), 2),
+                     ((16, 64, 32), 2)]:
+        if r == 4 and cap == "3":
+            continue  # would need more than 4 factors
+        P.check_against_oracle(emu, orc, shape, r, seed=int(cap))
+
+
+@pytest.mark.parametrize("dims,batch,base,form,per", [
+    ((1024,), 4, 2, 0, False), ((4 ** 7,), 2, 4, 0, True), ((64, 32), 3, 2, 1, False),
+    ((2 ** 14,), 2, 2, 1, True), ((16, 16, 16), 2, 4, 1, False), ((8 ** 3,), 2, 8, 0, False)])
+def test_native_conv(emu, dims, batch, base, form, per):
+    g = rng(21)
+    shape = (batch,) + dims
+    x = g.standard_normal(shape) + 1j * g.standard_normal(shape)
+    hs = shape if per else dims
+    h = g.standard_normal(hs) + 1j * g.standard_normal(hs)
+    y = P.native_conv(emu, dims, batch, base, form, x, h, per_problem=per)
+    axes = tuple(range(1, len(shape)))
+    z = P.fftconv(x, h if per else h[None], axes)
+    tol = P.TOL if form == 0 else P.TOL_F32
+    assert P.crel(y, z) < tol
+
+
+@pytest.mark.parametrize("op", [pac.OP_AT, pac.OP_A, pac.OP_CONJ_A, pac.OP_FFT, pac.OP_IFFT,
+                                pac.OP_UIFFT])
+@pytest.mark.parametrize("dims,base", [((4096,), 4), ((2 ** 13,), 2), ((64, 128), 2)])
+def test_native_transform(emu, orc, op, dims, base):
+    g = rng(4)
+    x = g.standard_normal((2,) + dims) + 1j * g.standard_normal((2,) + dims)
+    y = P.native_transform(emu, dims, 2, base, 0, op, x)
+    for b in range(2):
+        if op == pac.OP_FFT:
+            z = np.fft.fftn(x[b])
+        elif op == pac.OP_IFFT:
+            z = np.fft.ifftn(x[b])
+        else:
+            oop = {pac.OP_AT: O.OP_AT, pac.OP_A: O.OP_A, pac.OP_CONJ_A: O.OP_CONJ,
+                   pac.OP_UIFFT: O.OP_CONJ}[op]
+            zr, zi = orc.butterflies(oop, base, x[b].real, x[b].imag)
+            z = zr + 1j * zi
+            if op == pac.OP_UIFFT:
+                z = z / np.prod(dims)
+        assert P.crel(y[b], z) < P.TOL
+
+
+def test_invalid_size_leaves_data_untouched(emu):
+    g = rng(1)
+    x = g.standard_normal(48), g.standard_normal(48)
+    h = g.standard_normal(48), g.standard_normal(48)
+    y = pac.dropin_convolution(emu, 1, 2, *x, *h)
+    assert emu.pac_get_last_status() == 2
+    assert np.array_equal(y[0], x[0]) and np.array_equal(y[2], h[0])
+    # a power of 2 that is not a power of 4
+    x = g.standard_normal(32), g.standard_normal(32)
+    y = pac.dropin_butterflies(emu, 2, 4, *x)
+    assert emu.pac_get_last_status() == 2
+    assert np.array_equal(y[0], x[0])
+    # success clears nothing but reports success
+    y = pac.dropin_butterflies(emu, 2, 2, *x)
+    assert emu.pac_get_last_status() == 0
+
+
+def test_unsupported_radix_matches_reference_behaviour(emu, orc):
+    """3D r = 8 and 1D r = 3: the reference skips the butterflies."""
+    g = rng(2)
+    s = (8, 8, 8)
+    x = g.standard_normal(s), g.standard_normal(s)
+    h = g.standard_normal(s), g.standard_normal(s)
+    y = pac.dropin_convolution(emu, 1, 8, *x, *h)
+    z = orc.convolution(1, 8, *x, *h)
+    assert rel_l2(y[0], y[1], z[0], z[1]) < 1e-15
+    assert np.array_equal(y[2], h[0])
+    x = g.standard_normal(9), g.standard_normal(9)
+    h = g.standard_normal(9), g.standard_normal(9)
+    y = pac.dropin_convolution(emu, 1, 3, *x, *h)
+    z = (x[0] + 1j * x[1]) * (h[0] + 1j * h[1]) / 9
+    assert P.crel(y[0] + 1j * y[1], z) < 1e-15
+
+
+def test_twiddle_tables(emu, orc):
+    for r, n in ((2, 1024), (4, 4096), (8, 512), (4, 2048)):
+        a = pac.dropin_twiddles(emu, r, n)
+        b = orc.twiddles(r, n)
+        assert len(a) == len(b)
+        # the reference evaluates cos/sin of a rounded angle -2*pi*m*j/k, which
+        # carries up to ~|angle| * eps; the device tables use the exact
+        # fraction 2*m*j/k (sincospi), so they agree to a few 1e-16
+        for u, v in zip(a, b):
+            assert np.max(np.abs(u - v)) < 2e-15
+
+
+def test_index_reversal_tables(emu, orc):
+    import ctypes as C
+    for r, dims in ((2, (64,)), (4, (256,)), (8, (512,)), (2, (8, 32)), (4, (16, 64)),
+                    (2, (4, 8, 16)), (4, (16, 4, 64))):
+        n = int(np.prod(dims))
+        f = getattr(emu, f"precompute_index_reversal_permutation_r{r}"
+                    + ("" if len(dims) == 1 else f"_{len(dims)}d"))
+        p = f(*dims)
+        got = np.ctypeslib.as_array(p, shape=(n,)).copy()
+        C.CDLL(None).free(C.cast(p, C.c_void_p))
+        assert np.array_equal(got, orc.rho(r, dims))
+
+
+def test_standalone_permutation(emu, orc):
+    g = rng(8)
+    n = 1024
+    re, im = g.standard_normal(n), g.standard_normal(n)
+    rho = orc.rho(4, (n,))
+    a, b = re.copy(), im.copy()
+    import ctypes as C
+    emu.apply_permutation_split(a.ctypes.data_as(C.POINTER(C.c_double)),
+                                b.ctypes.data_as(C.POINTER(C.c_double)), n,
+                                rho.ctypes.data_as(C.POINTER(C.c_int)))
+    assert np.array_equal(a, re[rho]) and np.array_equal(b, im[rho])
+    z = np.stack([re, im], axis=1).copy()
+    emu.apply_permutation(z.ctypes.data_as(C.POINTER(C.c_double)), n,
+                          rho.ctypes.data_as(C.POINTER(C.c_int)))
+    assert np.array_equal(z[:, 0], re[rho]) and np.array_equal(z[:, 1], im[rho])

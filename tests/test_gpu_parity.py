@@ -1,0 +1,205 @@
+"""Parity of the sm_100a library (libpac.so) with the oracle, on the GPU.
+
+Every call goes through the C ABI: fft.h (host pointers, the reference's
+prototypes) or pac.h (plans, device pointers).  FP64 results must match the
+oracle to 1e-13 relative L2, the reference's digit-reversal order exactly
+(the overwritten filter A^T h is compared position by position), and the FP32
+form the FP64 oracle to 1e-6 relative L2.
+"""
+import importlib
+import threading
+
+import numpy as np
+import pytest
+
+import parity as P
+from conftest import O, pac, rel_l2, rng
+
+pytestmark = pytest.mark.gpu
+W = importlib.import_module("c-permutation-avoiding-convolution_b200.workloads")
+
+
+def test_golden(lib, golden):
+    P.check_golden(lib, golden)
+
+
+@pytest.mark.parametrize("shape,r", [
+    ((4096,), 4), ((4096,), 2), ((4096,), 8), ((8192,), 2), ((4 ** 8,), 4), ((8 ** 5,), 8),
+    ((2 ** 17,), 2), ((8192, 4), 2), ((4, 8192), 2), ((256, 256), 4), ((512, 64), 2),
+    ((64, 64, 64), 4), ((128, 4, 4), 2), ((16, 32, 64), 2), ((1,), 2), ((2,), 2), ((1,), 8)])
+def test_oracle_sizes(lib, orc, shape, r):
+    P.check_against_oracle(lib, orc, shape, r, ops=np.prod(shape) <= 2 ** 17)
+
+
+@pytest.mark.parametrize("cap", ["3", "4", "6"])
+def test_multi_factor_splits(lib, orc, cap, monkeypatch):
+    monkeypatch.setenv("PAC_MAX_FACTOR_LOG", cap)
+    for shape, r in [((2 ** 12,), 2), ((4 ** 6,), 4), ((8 ** 4,), 8), ((128, 32), 2),
+                     ((16, 64, 32), 2)]:
+        if r == 4 and cap == "3":
+            continue
+        P.check_against_oracle(lib, orc, shape, r, seed=int(cap))
+
+
+def test_c1_against_reference_and_direct_sum(lib, orc):
+    """C1: n = 2^12, radix 4, N(0,1) inputs."""
+    x, h = W.c1()
+    xs, hs = (x.real, x.imag), (h.real, h.imag)
+    y = pac.dropin_convolution(lib, O.METHOD_PAC, 4, *xs, *hs)
+    z = orc.convolution(O.METHOD_PAC, 4, *xs, *hs)
+    assert rel_l2(y[0], y[1], z[0], z[1]) < P.TOL
+    assert rel_l2(y[2], y[3], z[2], z[3]) < P.TOL
+    d = orc.naive_conv(*xs, *hs)
+    assert rel_l2(y[0], y[1], *d) < P.TOL
+    # the A^T x intermediate is the reference's element by element
+    a = pac.dropin_butterflies(lib, O.OP_AT, 4, *xs)
+    b = orc.butterflies(O.OP_AT, 4, *xs)
+    assert rel_l2(*a, *b) < P.TOL
+    for r in (2, 8):
+        y = pac.dropin_convolution(lib, O.METHOD_PAC, r, *xs, *hs)
+        assert rel_l2(y[0], y[1], *d) < P.TOL
+
+
+@pytest.mark.parametrize("form", [pac.PAC_FORM_F64, pac.PAC_FORM_F32])
+def test_c2_batched_1d(lib, orc, form):
+    """C2: 1024 x 2^16 with one 257-tap filter; sampled rows against the
+    oracle (reference radix 4, 2^16 = 4^8) and the whole batch through
+    linearity: sum_b (x_b * h) = (sum_b x_b) * h."""
+    x, h = W.c2()
+    y = P.native_conv(lib, (65536,), 1024, 2, form, x, h)
+    tol = P.TOL if form == pac.PAC_FORM_F64 else P.TOL_F32
+    for b in (0, 1, 511, 1023):
+        z = orc.convolution(O.METHOD_PAC, 4, x[b].real, x[b].imag, h.real, h.imag)
+        assert P.crel(y[b], z[0] + 1j * z[1]) < tol
+    s = x.sum(axis=0)
+    z = orc.convolution(O.METHOD_PAC, 4, s.real, s.imag, h.real, h.imag)
+    assert P.crel(y.sum(axis=0), z[0] + 1j * z[1]) < tol * 4
+
+
+@pytest.mark.parametrize("form", [pac.PAC_FORM_F64, pac.PAC_FORM_F32])
+def test_c3_2d(lib, orc, form):
+    """C3: 2048^2, Gaussian 31x31 filter; oracle at reference radix 2."""
+    x, h = W.c3()
+    y = P.native_conv(lib, (2048, 2048), 1, 2, form, x, h)[0]
+    z = orc.convolution(O.METHOD_PAC, 2, x.real, x.imag, h.real, h.imag)
+    tol = P.TOL if form == pac.PAC_FORM_F64 else P.TOL_F32
+    assert P.crel(y, z[0] + 1j * z[1]) < tol
+
+
+def test_c3_dropin_matches_reference_semantics(lib, orc):
+    x, h = W.c3()
+    y = pac.dropin_convolution(lib, O.METHOD_PAC, 2, x.real, x.imag, h.real, h.imag)
+    z = orc.convolution(O.METHOD_PAC, 2, x.real, x.imag, h.real, h.imag)
+    assert rel_l2(y[0], y[1], z[0], z[1]) < P.TOL
+    assert rel_l2(y[2], y[3], z[2], z[3]) < P.TOL
+
+
+@pytest.mark.parametrize("shape", [(256, 256, 256), (512, 256, 128)])
+def test_c4_3d_f32(lib, shape):
+    """C4 in FP32 against an FP64 reference (numpy.fft), plus the impulse
+    property at full size: x = delta gives y = h."""
+    x, h = W.c4(shape)
+    y = P.native_conv(lib, shape, 1, 2, pac.PAC_FORM_F32, x, h)[0]
+    z = P.fftconv(x, h, (0, 1, 2))
+    assert P.crel(y, z) < P.TOL_F32
+    d = np.zeros(shape, np.complex128)
+    d[0, 0, 0] = 1.0
+    y = P.native_conv(lib, shape, 1, 2, pac.PAC_FORM_F32, d, h)[0]
+    assert P.crel(y, h) < P.TOL_F32
+
+
+def test_c4_3d_f64_against_oracle(lib, orc):
+    shape = (64, 128, 32)
+    x, h = W.c4(shape)
+    y = P.native_conv(lib, shape, 1, 2, pac.PAC_FORM_F64, x, h)[0]
+    z = orc.convolution(O.METHOD_PAC, 2, x.real, x.imag, h.real, h.imag)
+    assert P.crel(y, z[0] + 1j * z[1]) < P.TOL
+
+
+@pytest.mark.parametrize("dims,batch,base,form,per", [
+    ((1024,), 4, 2, 0, False), ((4 ** 7,), 2, 4, 0, True), ((64, 32), 3, 2, 1, False),
+    ((2 ** 14,), 2, 2, 1, True), ((16, 16, 16), 2, 4, 1, False), ((8 ** 3,), 2, 8, 0, False),
+    ((2 ** 20,), 2, 2, 0, False), ((2 ** 20,), 2, 2, 1, False)])
+def test_native_conv(lib, dims, batch, base, form, per):
+    g = rng(21)
+    shape = (batch,) + dims
+    x = g.standard_normal(shape) + 1j * g.standard_normal(shape)
+    hs = shape if per else dims
+    h = g.standard_normal(hs) + 1j * g.standard_normal(hs)
+    y = P.native_conv(lib, dims, batch, base, form, x, h, per_problem=per)
+    z = P.fftconv(x, h if per else h[None], tuple(range(1, len(shape))))
+    assert P.crel(y, z) < (P.TOL if form == 0 else P.TOL_F32)
+
+
+@pytest.mark.parametrize("op", [pac.OP_AT, pac.OP_A, pac.OP_CONJ_A, pac.OP_FFT, pac.OP_IFFT,
+                                pac.OP_UIFFT])
+@pytest.mark.parametrize("dims,base", [((4096,), 4), ((2 ** 13,), 2), ((64, 128), 2),
+                                       ((2 ** 16,), 4)])
+def test_native_transform(lib, orc, op, dims, base):
+    g = rng(4)
+    x = g.standard_normal((2,) + dims) + 1j * g.standard_normal((2,) + dims)
+    y = P.native_transform(lib, dims, 2, base, 0, op, x)
+    for b in range(2):
+        if op == pac.OP_FFT:
+            z = np.fft.fftn(x[b])
+        elif op == pac.OP_IFFT:
+            z = np.fft.ifftn(x[b])
+        else:
+            oop = {pac.OP_AT: O.OP_AT, pac.OP_A: O.OP_A, pac.OP_CONJ_A: O.OP_CONJ,
+                   pac.OP_UIFFT: O.OP_CONJ}[op]
+            zr, zi = orc.butterflies(oop, base, x[b].real, x[b].imag)
+            z = (zr + 1j * zi) / (np.prod(dims) if op == pac.OP_UIFFT else 1)
+        assert P.crel(y[b], z) < P.TOL
+
+
+def test_invalid_inputs_leave_data_untouched(lib):
+    g = rng(1)
+    x = g.standard_normal(48), g.standard_normal(48)
+    h = g.standard_normal(48), g.standard_normal(48)
+    y = pac.dropin_convolution(lib, 1, 2, *x, *h)
+    assert lib.pac_get_last_status() == 2
+    assert np.array_equal(y[0], x[0]) and np.array_equal(y[2], h[0])
+    x = g.standard_normal(32), g.standard_normal(32)
+    y = pac.dropin_butterflies(lib, 2, 4, *x)
+    assert lib.pac_get_last_status() == 2 and np.array_equal(y[0], x[0])
+    y = pac.dropin_butterflies(lib, 2, 2, *x)
+    assert lib.pac_get_last_status() == 0
+
+
+def test_unsupported_radix_behaviour(lib, orc):
+    g = rng(2)
+    s = (16, 16)
+    x = g.standard_normal(s), g.standard_normal(s)
+    h = g.standard_normal(s), g.standard_normal(s)
+    y = pac.dropin_convolution(lib, 1, 8, *x, *h)
+    z = orc.convolution(1, 8, *x, *h)
+    assert rel_l2(y[0], y[1], z[0], z[1]) < 1e-15 and np.array_equal(y[2], h[0])
+
+
+def test_twiddle_tables(lib, orc):
+    for r, n in ((2, 1024), (4, 4096), (8, 512), (4, 2048)):
+        a = pac.dropin_twiddles(lib, r, n)
+        b = orc.twiddles(r, n)
+        assert len(a) == len(b)
+        for u, v in zip(a, b):
+            assert np.max(np.abs(u - v)) < 2e-15
+
+
+def test_concurrent_callers(lib, orc):
+    """Two host threads on different shapes and one shape shared."""
+    errs = []
+
+    def work(shape, r, seed):
+        try:
+            for k in range(3):
+                P.check_against_oracle(lib, orc, shape, r, seed=seed + k, ops=False)
+        except AssertionError as e:  # pragma: no cover
+            errs.append(e)
+
+    ts = [threading.Thread(target=work, args=a) for a in
+          (((4096,), 4, 1), ((64, 64), 2, 2), ((4096,), 4, 3))]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+    assert not errs, errs
