@@ -267,18 +267,25 @@ int be_stream_wait(void* waiter, void* waitee) {
 template <typename T, int B2>
 static int launch_pass_t(const PassDesc& d, long long grid, int threads, size_t smem,
                          void* stream) {
+  // opt the kernel into the device's whole shared-memory budget once per
+  // device, so that every pass geometry (<= 200 KiB) launches
   static std::mutex mu;
-  static std::set<std::pair<int, size_t>> configured;
+  static std::set<int> configured;
   auto kern = pac_pass_kernel<T, B2>;
   if (smem > 48 * 1024) {
     int dev = 0;
     cudaGetDevice(&dev);
     std::lock_guard<std::mutex> g(mu);
-    auto key = std::make_pair(dev, smem);
-    if (!configured.count(key)) {
-      PAC_CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+    if (!configured.count(dev)) {
+      int optin = 0;
+      PAC_CU(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev),
+             "cudaDeviceGetAttribute");
+      cudaFuncAttributes fa;
+      PAC_CU(cudaFuncGetAttributes(&fa, kern), "cudaFuncGetAttributes");
+      PAC_CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  optin - (int)fa.sharedSizeBytes),
              "cudaFuncSetAttribute");
-      configured.insert(key);
+      configured.insert(dev);
     }
   }
   if (grid > 0x7fffffffLL) return set_error(PAC_ERROR_SIZE, "pass grid too large");

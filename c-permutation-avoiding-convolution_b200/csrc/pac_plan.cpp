@@ -254,7 +254,10 @@ static PassSpec make_pass(const Schedule& s, int vi, long long batch, long long 
   if (wmax < 1) wmax = 1;
   while (W > wmax) W >>= 1;
   if (W > 64) W = 64;
-  while (W > d.nlines) W >>= 1;
+  // tiles must cover the lines exactly: W divides nlines (a batch that is
+  // not a power of two makes nlines odd-factored)
+  const long long lowbit = d.nlines & -d.nlines;
+  if (W > lowbit) W = lowbit;
   if (W < 1) W = 1;
   d.W = (int)W;
   d.logW = 0;
