@@ -376,6 +376,46 @@ def run_ours(args, world, dist):
     return out
 
 
+def run_profile(args):
+    """Lean run for ncu: 2 pac_pass_kernel launches of the filter spectrum (2D),
+    then warm-up and timed convolutions, nothing else on the device."""
+    import torch
+
+    cfg = CONFIGS[args.config]
+    dims, batch = cfg["dims"], cfg["batch"]
+    form = pac.PAC_FORM_F64 if args.form == "f64" else pac.PAC_FORM_F32
+    tdt = torch.float64 if form == pac.PAC_FORM_F64 else torch.float32
+    dev = torch.device("cuda", 0)
+    L = pac.load()
+    x, h = make_inputs(args.config)
+    x = x.reshape((batch,) + dims)
+    h = h.reshape(dims)
+
+    def t(a, dt):
+        return torch.from_numpy(np.ascontiguousarray(a)).to(dev).to(dt)
+
+    xs = [(t(x.real, tdt), t(x.imag, tdt)) for _ in range(2)]
+    hd = (t(h.real, torch.float64), t(h.imag, torch.float64))
+    Hh = (torch.empty(dims, dtype=tdt, device=dev), torch.empty(dims, dtype=tdt, device=dev))
+    y = (torch.empty_like(xs[0][0]), torch.empty_like(xs[0][1]))
+    sp = torch.cuda.current_stream(dev).cuda_stream
+    plan = pac.Plan(L, dims, batch, 2, form)
+    plan.filter_spectrum(hd[0].data_ptr(), hd[1].data_ptr(), Hh[0].data_ptr(), Hh[1].data_ptr(),
+                         stream=sp)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for k in range(args.warmup + args.steps):
+        if k == args.warmup:
+            ev0.record()
+        a = xs[k % 2]
+        plan.convolve(a[0].data_ptr(), a[1].data_ptr(), Hh[0].data_ptr(), Hh[1].data_ptr(),
+                      y[0].data_ptr(), y[1].data_ptr(), stream=sp)
+    ev1.record()
+    torch.cuda.synchronize()
+    plan.close()
+    return {"mode": "profile", "config": args.config, "form": args.form,
+            "ms_per_step": ev0.elapsed_time(ev1) / max(args.steps, 1)}
+
+
 def run_e2e(args, world, dist):
     """The reference-facing call on pinned host buffers: H2D, transforms, D2H."""
     import ctypes as C
@@ -472,10 +512,16 @@ def main():
     ap.add_argument("--form", choices=["f64", "f32"], default="f64")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--no-forms", action="store_true", help="skip the FP32 comparison")
+    ap.add_argument("--profile", action="store_true",
+                    help="capture mode for ncu: filter spectrum, warm-up and timed steps only "
+                         "(two input buffers, no clock soak, e2e, CPU or FP32 legs)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
+    if args.profile:
+        print(json.dumps(run_profile(args)), flush=True)
+        return 0
 
     if args.impl == "reference":
         if rank == 0:
