@@ -19,6 +19,7 @@
 
 #include "pac.h"
 #include "pac_backend.h"
+#include "pac_special.h"
 
 namespace pac {
 
@@ -57,6 +58,23 @@ __global__ void __launch_bounds__(256) pac_pass_kernel(const PassDesc d) {
   }
   __syncthreads();
   pass_body<T, B2>(d, cta, sre, sim, s_lb, s_lb + 64);
+}
+
+// A pass compiled for one geometry (pac_special.h): tile W = 2^LOGW lines of
+// 2^LOGL elements, NT threads, register bound for MINB CTAs per SM.
+template <typename T, int B2, int MODE, int SIGN, int LOGL, int COLS, int LOGW, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) pac_special_kernel(const PassDesc d) {
+  constexpr int W = 1 << LOGW;
+  constexpr int PITCH = pitch_for((int)sizeof(T), LOGL, W);
+  using SP = Shape<LOGL, LOGW, PITCH, COLS>;
+  extern __shared__ __align__(16) unsigned char pac_smem[];
+  __shared__ long long s_lb[W];
+  T* sre = reinterpret_cast<T*>(pac_smem);
+  T* sim = sre + (size_t)W * PITCH;
+  const long long cta = blockIdx.x;
+  if ((int)threadIdx.x < W) s_lb[threadIdx.x] = line_base(d, cta * W + threadIdx.x);
+  __syncthreads();
+  pass_body_ct<T, B2, MODE, SIGN, SP, NT, RadsFor<LOGL, B2>>(d, cta, sre, sim, s_lb, s_lb);
 }
 
 template <typename T>
@@ -295,8 +313,57 @@ static int launch_pass_t(const PassDesc& d, long long grid, int threads, size_t 
   return PAC_SUCCESS;
 }
 
+template <typename K>
+static int launch_kernel(K kern, const PassDesc& d, long long grid, int threads, size_t smem,
+                         void* stream, std::set<int>& configured, std::mutex& mu) {
+  if (smem > 48 * 1024) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> g(mu);
+    if (!configured.count(dev)) {
+      int optin = 0;
+      PAC_CU(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev),
+             "cudaDeviceGetAttribute");
+      cudaFuncAttributes fa;
+      PAC_CU(cudaFuncGetAttributes(&fa, kern), "cudaFuncGetAttributes");
+      PAC_CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  optin - (int)fa.sharedSizeBytes),
+             "cudaFuncSetAttribute");
+      configured.insert(dev);
+    }
+  }
+  if (grid > 0x7fffffffLL) return set_error(PAC_ERROR_SIZE, "pass grid too large");
+  kern<<<(unsigned)grid, threads, smem, (cudaStream_t)stream>>>(d);
+  PAC_CU(cudaGetLastError(), "pac_special_kernel launch");
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return PAC_SUCCESS;
+}
+
+static int launch_special(const PassDesc& d, int elem_bytes, int b2, long long grid, int threads,
+                          size_t smem, void* stream, bool* done) {
+  *done = false;
+  const int cols = d.logS > 0 ? 1 : 0;
+#define PAC_X(T, BY, B2_, MO, SG, LL, CO, LW, NT_, MB)                                        \
+  if (!*done && elem_bytes == BY && b2 == B2_ && d.mode == MO &&                           \
+      (MO == MODE_CONV || d.sign == SG) && d.logL == LL && cols == CO && d.W == (1 << LW) && \
+      threads == NT_) {                                                                    \
+    static std::mutex mu;                                                                  \
+    static std::set<int> configured;                                                       \
+    *done = true;                                                                          \
+    return launch_kernel(pac_special_kernel<T, B2_, MO, SG, LL, CO, LW, NT_, MB>, d, grid,  \
+                         threads, smem, stream, configured, mu);                           \
+  }
+  PAC_SPECIAL_LIST(PAC_X)
+#undef PAC_X
+  return set_error(PAC_ERROR_INTERNAL, "no specialised kernel for a pass marked special");
+}
+
 int be_launch_pass(const PassDesc& d, int elem_bytes, int b2, long long grid, int threads,
                    size_t smem, void* stream) {
+  if (d.spec) {
+    bool done = false;
+    return launch_special(d, elem_bytes, b2, grid, threads, smem, stream, &done);
+  }
   if (elem_bytes == 8) {
     if (b2 == 1) return launch_pass_t<double, 1>(d, grid, threads, smem, stream);
     if (b2 == 2) return launch_pass_t<double, 2>(d, grid, threads, smem, stream);

@@ -16,6 +16,7 @@
 
 #include "pac.h"
 #include "pac_backend.h"
+#include "pac_special.h"
 
 namespace pac {
 
@@ -74,8 +75,37 @@ static void replay(const PassDesc& d, long long grid) {
   }
 }
 
-int be_launch_pass(const PassDesc& d, int elem_bytes, int b2, long long grid, int, size_t,
-                   void*) {
+// replay of a specialised kernel (pac_special.h): the compile-time body
+template <typename T, int B2, int MODE, int SIGN, int LOGL, int COLS, int LOGW, int NT>
+static void replay_special(const PassDesc& d, long long grid) {
+  constexpr int W = 1 << LOGW;
+  constexpr int PITCH = pitch_for((int)sizeof(T), LOGL, W);
+  using SP = Shape<LOGL, LOGW, PITCH, COLS>;
+  std::vector<T> sm((size_t)2 * W * PITCH);
+  std::vector<long long> lb(W);
+  for (long long cta = 0; cta < grid; ++cta) {
+    for (int w = 0; w < W; ++w) lb[w] = line_base(d, cta * W + w);
+    pass_body_ct<T, B2, MODE, SIGN, SP, NT, RadsFor<LOGL, B2>>(d, cta, sm.data(),
+                                                               sm.data() + (size_t)W * PITCH,
+                                                               lb.data(), lb.data());
+  }
+}
+
+int be_launch_pass(const PassDesc& d, int elem_bytes, int b2, long long grid, int threads,
+                   size_t, void*) {
+  if (d.spec) {
+    const int cols = d.logS > 0 ? 1 : 0;
+#define PAC_X(T, BY, B2_, MO, SG, LL, CO, LW, NT_, MB)                                        \
+  if (elem_bytes == BY && b2 == B2_ && d.mode == MO && (MO == MODE_CONV || d.sign == SG) && \
+      d.logL == LL && cols == CO && d.W == (1 << LW) && threads == NT_) {                  \
+    replay_special<T, B2_, MO, SG, LL, CO, LW, NT_>(d, grid);                              \
+    g_launches++;                                                                          \
+    return PAC_SUCCESS;                                                                    \
+  }
+    PAC_SPECIAL_LIST(PAC_X)
+#undef PAC_X
+    return set_error(PAC_ERROR_INTERNAL, "no specialised replay for a pass marked special");
+  }
   if (d.W > 64) return set_error(PAC_ERROR_INTERNAL, "W > 64");
   if (elem_bytes == 8) {
     if (b2 == 1) replay<double, 1>(d, grid);

@@ -83,6 +83,8 @@ struct PassDesc {
   int nat_Mlog;
   // device status word (bounded waits report here); may be null
   int* status;
+  // 1: this pass runs the kernel specialised for its geometry (pac_special.h)
+  int spec;
 };
 
 // ---------------------------------------------------------------------------
@@ -324,358 +326,5 @@ PAC_HD void nat_line(const PassDesc& d, long long g, long long* in_base, long lo
   *out_base = (o_real << (Mlog + d.logL + d.logS)) + ((long long)c << d.logS) + i;
 }
 
-// ---------------------------------------------------------------------------
-// One radix-R butterfly of a stage.
-//   DIF: load x[m] @ j + ell*m, DFT, twiddle output s by w_K^{j s},
-//        store @ j + ell*sigma_b(s)
-//   DIT: load x[s] @ j + ell*sigma_b(s), twiddle by w_K^{j s}, DFT,
-//        store @ j + ell*m
-// Global-facing stages read (first) or write (last) the line in global
-// memory; all other accesses go to the padded shared-memory line.
-// ---------------------------------------------------------------------------
-enum { IO_SMEM = 0, IO_GLOBAL = 1 };
-
-struct StageGeo {
-  int logK, logR, logell;
-  int twoff;
-};
-
-// butterfly index -> (w, blk, j)
-PAC_HD void bf_coords(const PassDesc& d, const StageGeo& st, bool global_facing, int u, int* w,
-                      int* blk, int* j) {
-  const int lbf = d.logL - st.logR;  // butterflies per line (log)
-  int v;
-  if (global_facing && d.logS > 0) {
-    *w = u & (d.W - 1);
-    v = u >> d.logW;
-  } else {
-    v = u & ((1 << lbf) - 1);
-    *w = u >> lbf;
-  }
-  *blk = v >> st.logell;
-  *j = v & ((1 << st.logell) - 1);
-}
-
-template <typename T, int B2, int R, int SIGN, bool DIF>
-PAC_HD void stage_bf(const PassDesc& d, long long cta, T* sre, T* sim, const StageGeo& st,
-                     int src, int dst, int u, const long long* lbase_in,
-                     const long long* lbase_out) {
-  constexpr int LR = ilog2(R);
-  static_assert(LR % B2 == 0, "radix must be a power of the digit base");
-  int w, blk, j;
-  bf_coords(d, st, src == IO_GLOBAL || dst == IO_GLOBAL, u, &w, &blk, &j);
-  const int ell = 1 << st.logell;
-  const int e0 = (blk << st.logK) + j;
-  const T* ire = (const T*)d.in_re;
-  const T* iim = (const T*)d.in_im;
-  Cx<T> x[R];
-  // ---- load
-  static_for<R>([&](auto mm) {
-    constexpr int m = mm.value;
-    constexpr int slot = DIF ? m : drev_c(m, LR, B2);
-    const int e = e0 + ell * slot;
-    if (src == IO_GLOBAL) {
-      long long gi = lbase_in[w] + ((long long)e << d.logS);
-      x[m] = Cx<T>{ld_g(ire + gi), ld_g(iim + gi)};
-    } else {
-      int si = w * d.pitch + sidx<T>(e);
-      x[m] = Cx<T>{sre[si], sim[si]};
-    }
-  });
-  const Cx<T>* tw = (const Cx<T>*)d.tw + st.twoff + j * (R - 1);
-  const bool twiddle = st.logell > 0 && j > 0;
-  // ---- DIT: 4-step pre-twiddle (first DIT stage only, ell == 1) and
-  //      stage twiddle on the inputs
-  if constexpr (!DIF) {
-    if (d.tw4 == 2 && st.logell == 0) {
-      long long g = (long long)cta * d.W + w;
-      long long i = g & ((1LL << d.logS) - 1);
-      uint32_t iG = (uint32_t)((i >> d.tw4_shift) & d.tw4_mask);
-      const Cx<T>* lo = (const Cx<T>*)d.tw4_lo;
-      const Cx<T>* hi = (const Cx<T>*)d.tw4_hi;
-      static_for<R>([&](auto mm) {
-        constexpr int m = mm.value;
-        constexpr int slot = drev_c(m, LR, B2);
-        uint32_t E = iG * drev<B2>((uint32_t)(e0 + slot), d.logL);
-        Cx<T> wv = cmul(ld_tw(lo + (E & ((1u << d.tw4_lolog) - 1))), ld_tw(hi + (E >> d.tw4_lolog)));
-        x[m] = ctw(x[m], wv, SIGN);
-      });
-    }
-    if (twiddle) {
-      static_for<R - 1>([&](auto ss) {
-        constexpr int s = ss.value + 1;
-        x[s] = ctw(x[s], ld_tw(tw + (s - 1)), SIGN);
-      });
-    }
-  }
-  dft_reg<T, R, SIGN>(x);
-  // register p now holds output index brev(p)
-  if constexpr (DIF) {
-    if (twiddle) {
-      static_for<R>([&](auto pp) {
-        constexpr int s = brev_c(pp.value, LR);
-        if constexpr (s > 0) x[pp.value] = ctw(x[pp.value], ld_tw(tw + (s - 1)), SIGN);
-      });
-    }
-    if (d.tw4 == 1 && st.logell == 0) {
-      long long g = (long long)cta * d.W + w;
-      long long i = g & ((1LL << d.logS) - 1);
-      uint32_t iG = (uint32_t)((i >> d.tw4_shift) & d.tw4_mask);
-      const Cx<T>* lo = (const Cx<T>*)d.tw4_lo;
-      const Cx<T>* hi = (const Cx<T>*)d.tw4_hi;
-      static_for<R>([&](auto pp) {
-        constexpr int slot = drev_c(brev_c(pp.value, LR), LR, B2);
-        uint32_t E = iG * drev<B2>((uint32_t)(e0 + ell * slot), d.logL);
-        Cx<T> wv = cmul(ld_tw(lo + (E & ((1u << d.tw4_lolog) - 1))), ld_tw(hi + (E >> d.tw4_lolog)));
-        x[pp.value] = ctw(x[pp.value], wv, SIGN);
-      });
-    }
-  }
-  // ---- store
-  T* ore = (T*)d.out_re;
-  T* oim = (T*)d.out_im;
-  static_for<R>([&](auto pp) {
-    constexpr int p = pp.value;
-    constexpr int slot = DIF ? drev_c(brev_c(p, LR), LR, B2) : brev_c(p, LR);
-    const int e = e0 + ell * slot;
-    Cx<T> v = x[p];
-    if (dst == IO_GLOBAL) {
-      if (d.use_scale) {
-        v.re *= T(d.scale);
-        v.im *= T(d.scale);
-      }
-      long long gi = lbase_out[w] + ((long long)e << d.logS);
-      ore[gi] = v.re;
-      oim[gi] = v.im;
-    } else {
-      int si = w * d.pitch + sidx<T>(e);
-      sre[si] = v.re;
-      sim[si] = v.im;
-    }
-  });
-}
-
-// Convolution middle: the last DIF stage (ell == 1), the pointwise product
-// with the filter spectrum at the same P_b positions, and the first DIT
-// stage, all in registers.
-template <typename T, int B2, int R>
-PAC_HD void middle_bf(const PassDesc& d, long long cta, T* sre, T* sim, const StageGeo& st,
-                      int src, int dst, int u, const long long* lbase) {
-  constexpr int LR = ilog2(R);
-  int w, blk, j;
-  bf_coords(d, st, src == IO_GLOBAL || dst == IO_GLOBAL, u, &w, &blk, &j);
-  const int e0 = blk << st.logK;  // ell == 1, j == 0
-  const T* ire = (const T*)d.in_re;
-  const T* iim = (const T*)d.in_im;
-  const T* hre = (const T*)d.h_re;
-  const T* him = (const T*)d.h_im;
-  Cx<T> x[R];
-  static_for<R>([&](auto mm) {
-    constexpr int m = mm.value;
-    const int e = e0 + m;
-    if (src == IO_GLOBAL) {
-      long long gi = lbase[w] + ((long long)e << d.logS);
-      x[m] = Cx<T>{ld_g(ire + gi), ld_g(iim + gi)};
-    } else {
-      int si = w * d.pitch + sidx<T>(e);
-      x[m] = Cx<T>{sre[si], sim[si]};
-    }
-  });
-  dft_reg<T, R, -1>(x);
-  // register p holds the spectrum at slot sigma_b(brev(p)); the DIT stage
-  // wants register s = the value at slot sigma_b(s), i.e. register brev(s).
-  Cx<T> y[R];
-  const T sc = T(d.scale);
-  static_for<R>([&](auto ss) {
-    constexpr int s = ss.value;
-    constexpr int p = brev_c(s, LR);
-    const int e = e0 + drev_c(s, LR, B2);
-    long long hi = (lbase[w] + ((long long)e << d.logS)) & d.h_mask;
-    Cx<T> hv = Cx<T>{ld_g(hre + hi) * sc, ld_g(him + hi) * sc};
-    y[s] = cmul(x[p], hv);
-  });
-  dft_reg<T, R, +1>(y);
-  T* ore = (T*)d.out_re;
-  T* oim = (T*)d.out_im;
-  static_for<R>([&](auto pp) {
-    constexpr int p = pp.value;
-    const int e = e0 + brev_c(p, LR);
-    if (dst == IO_GLOBAL) {
-      long long gi = lbase[w] + ((long long)e << d.logS);
-      ore[gi] = y[p].re;
-      oim[gi] = y[p].im;
-    } else {
-      int si = w * d.pitch + sidx<T>(e);
-      sre[si] = y[p].re;
-      sim[si] = y[p].im;
-    }
-  });
-}
-
-// ---------------------------------------------------------------------------
-// Runtime -> compile-time dispatch of one butterfly
-// ---------------------------------------------------------------------------
-template <typename T, int B2, bool DIF>
-PAC_HD void stage_dispatch(const PassDesc& d, long long cta, T* sre, T* sim, const StageGeo& st,
-                           int sign, int src, int dst, int u, const long long* lbi,
-                           const long long* lbo) {
-#define PAC_ST(RR)                                                                          \
-  if (sign < 0) stage_bf<T, B2, RR, -1, DIF>(d, cta, sre, sim, st, src, dst, u, lbi, lbo); \
-  else stage_bf<T, B2, RR, +1, DIF>(d, cta, sre, sim, st, src, dst, u, lbi, lbo);
-  if constexpr (B2 == 1) {
-    switch (st.logR) {
-      case 1: PAC_ST(2) break;
-      case 2: PAC_ST(4) break;
-      case 3: PAC_ST(8) break;
-      default: PAC_ST(16) break;
-    }
-  } else if constexpr (B2 == 2) {
-    if (st.logR == 2) { PAC_ST(4) } else { PAC_ST(16) }
-  } else {
-    PAC_ST(8)
-  }
-#undef PAC_ST
-}
-
-template <typename T, int B2>
-PAC_HD void middle_dispatch(const PassDesc& d, long long cta, T* sre, T* sim, const StageGeo& st,
-                            int src, int dst, int u, const long long* lb) {
-  if constexpr (B2 == 1) {
-    switch (st.logR) {
-      case 1: middle_bf<T, B2, 2>(d, cta, sre, sim, st, src, dst, u, lb); break;
-      case 2: middle_bf<T, B2, 4>(d, cta, sre, sim, st, src, dst, u, lb); break;
-      case 3: middle_bf<T, B2, 8>(d, cta, sre, sim, st, src, dst, u, lb); break;
-      default: middle_bf<T, B2, 16>(d, cta, sre, sim, st, src, dst, u, lb); break;
-    }
-  } else if constexpr (B2 == 2) {
-    if (st.logR == 2) middle_bf<T, B2, 4>(d, cta, sre, sim, st, src, dst, u, lb);
-    else middle_bf<T, B2, 16>(d, cta, sre, sim, st, src, dst, u, lb);
-  } else {
-    middle_bf<T, B2, 8>(d, cta, sre, sim, st, src, dst, u, lb);
-  }
-}
-
-// ---------------------------------------------------------------------------
-// Pass body: a sequence of phases separated by CTA barriers.  A phase is a
-// loop over butterflies; the device runs it with one butterfly per thread,
-// the host emulator with a plain loop.  Barrier placement: every phase that
-// reads shared memory is preceded by a barrier after the phase that wrote it.
-// ---------------------------------------------------------------------------
-#if defined(__CUDA_ARCH__)
-#define PAC_FOR_BF(n, u) for (int u = (int)threadIdx.x; u < (n); u += (int)blockDim.x)
-#define PAC_SYNC() __syncthreads()
-#else
-#define PAC_FOR_BF(n, u) for (int u = 0; u < (n); ++u)
-#define PAC_SYNC() ((void)0)
-#endif
-
-PAC_HD StageGeo geo_of(const PassDesc& d, int i) {
-  // stage i of the DIF order: K_i = L / (R_0 ... R_{i-1})
-  int logK = d.logL;
-  for (int q = 0; q < i; ++q) logK -= d.rlog[q];
-  StageGeo g;
-  g.logK = logK;
-  g.logR = d.rlog[i];
-  g.logell = logK - d.rlog[i];
-  g.twoff = d.tw_off[i];
-  return g;
-}
-
-template <typename T, int B2>
-PAC_HD void pass_body(const PassDesc& d, long long cta, T* sre, T* sim, long long* lbi,
-                      long long* lbo) {
-  // per-line global bases (W <= 64); every thread computes them
-  const bool nat = d.nat != 0;
-  for (int w = 0; w < d.W; ++w) {
-    long long g = cta * d.W + w;
-    if (nat) {
-      nat_line<B2>(d, g, &lbi[w], &lbo[w]);
-    } else {
-      lbi[w] = line_base(d, g);
-      lbo[w] = lbi[w];
-    }
-  }
-  const int nst = d.nst;
-  if (d.mode == MODE_DIF) {
-    for (int i = 0; i < nst; ++i) {
-      StageGeo st = geo_of(d, i);
-      int src = (i == 0) ? IO_GLOBAL : IO_SMEM;
-      int dst = (i == nst - 1 && !nat) ? IO_GLOBAL : IO_SMEM;
-      int nbf = d.W << (d.logL - st.logR);
-      if (i > 0) PAC_SYNC();
-      PAC_FOR_BF(nbf, u) {
-        stage_dispatch<T, B2, true>(d, cta, sre, sim, st, d.sign, src, dst, u, lbi, lbo);
-      }
-    }
-    if (nat) {
-      // natural-order store out of shared memory
-      PAC_SYNC();
-      T* ore = (T*)d.out_re;
-      T* oim = (T*)d.out_im;
-      const int n = d.W << d.logL;
-      const bool lines_fast = d.logS > 0 || d.nat_nf > 0;
-      PAC_FOR_BF(n, u) {
-        int w, q;
-        if (lines_fast) {
-          w = u & (d.W - 1);
-          q = u >> d.logW;
-        } else {
-          w = u >> d.logL;
-          q = u & (d.L - 1);
-        }
-        // q is the natural index inside this factor: it sits at slot rev(q)
-        int e = (int)drev<B2>((uint32_t)q, d.logL);
-        int si = w * d.pitch + sidx<T>(e);
-        T vr = sre[si], vi = sim[si];
-        if (d.use_scale) {
-          vr *= T(d.scale);
-          vi *= T(d.scale);
-        }
-        long long gi = lbo[w] + ((long long)q << (d.nat_Mlog + d.logS));
-        ore[gi] = vr;
-        oim[gi] = vi;
-      }
-    }
-  } else if (d.mode == MODE_DIT) {
-    for (int k = 0; k < nst; ++k) {
-      int i = nst - 1 - k;
-      StageGeo st = geo_of(d, i);
-      int src = (k == 0) ? IO_GLOBAL : IO_SMEM;
-      int dst = (k == nst - 1) ? IO_GLOBAL : IO_SMEM;
-      int nbf = d.W << (d.logL - st.logR);
-      if (k > 0) PAC_SYNC();
-      PAC_FOR_BF(nbf, u) {
-        stage_dispatch<T, B2, false>(d, cta, sre, sim, st, d.sign, src, dst, u, lbi, lbo);
-      }
-    }
-  } else {  // MODE_CONV
-    for (int i = 0; i < nst - 1; ++i) {
-      StageGeo st = geo_of(d, i);
-      int src = (i == 0) ? IO_GLOBAL : IO_SMEM;
-      int nbf = d.W << (d.logL - st.logR);
-      if (i > 0) PAC_SYNC();
-      PAC_FOR_BF(nbf, u) {
-        stage_dispatch<T, B2, true>(d, cta, sre, sim, st, -1, src, IO_SMEM, u, lbi, lbo);
-      }
-    }
-    {
-      StageGeo st = geo_of(d, nst - 1);
-      int src = (nst == 1) ? IO_GLOBAL : IO_SMEM;
-      int dst = (nst == 1) ? IO_GLOBAL : IO_SMEM;
-      int nbf = d.W << (d.logL - st.logR);
-      if (nst > 1) PAC_SYNC();
-      PAC_FOR_BF(nbf, u) { middle_dispatch<T, B2>(d, cta, sre, sim, st, src, dst, u, lbi); }
-    }
-    for (int i = nst - 2; i >= 0; --i) {
-      StageGeo st = geo_of(d, i);
-      int dst = (i == 0) ? IO_GLOBAL : IO_SMEM;
-      int nbf = d.W << (d.logL - st.logR);
-      PAC_SYNC();
-      PAC_FOR_BF(nbf, u) {
-        stage_dispatch<T, B2, false>(d, cta, sre, sim, st, +1, IO_SMEM, dst, u, lbi, lbo);
-      }
-    }
-  }
-}
-
 }  // namespace pac
+#include "pac_stages.cuh"

@@ -35,6 +35,7 @@
 
 #include "pac.h"
 #include "pac_backend.h"
+#include "pac_special.h"
 
 namespace pac {
 
@@ -91,26 +92,11 @@ struct Schedule {
 
 static const int kSmemBudget = 200 * 1024;
 
-// stage radices of one factor of length 2^lg for digit base 2^b2
+// stage radices of one factor of length 2^lg for digit base 2^b2 (the same
+// schedule the specialised kernels are compiled with, pac_special.h)
 static std::vector<int> radix_schedule(int lg, int b2) {
   std::vector<int> r;
-  if (b2 == 3) {
-    for (int i = 0; i < lg; i += 3) r.push_back(3);
-  } else if (b2 == 2) {
-    int x = lg;
-    while (x >= 4) {
-      r.push_back(4);
-      x -= 4;
-    }
-    if (x) r.push_back(2);
-  } else {
-    int x = lg;
-    while (x >= 4) {
-      r.push_back(4);
-      x -= 4;
-    }
-    if (x) r.push_back(x);
-  }
+  for (int i = 0; i < sched_n(lg, b2); ++i) r.push_back(sched_v(lg, b2, i));
   return r;
 }
 
@@ -262,12 +248,7 @@ static PassSpec make_pass(const Schedule& s, int vi, long long batch, long long 
   d.W = (int)W;
   d.logW = 0;
   while ((1 << d.logW) < d.W) ++d.logW;
-  int pitch = base_pitch;
-  if (d.W > 1) {
-    int want = (NB / (d.W < NB ? d.W : NB)) % NB;
-    pitch += ((want - pitch % NB) % NB + NB) % NB;
-  }
-  d.pitch = pitch;
+  d.pitch = pitch_for(esz, v.log, d.W);
   const std::vector<int>& rad = s.rad[vi];
   d.nst = (int)rad.size();
   int logK = v.log;
@@ -305,6 +286,27 @@ static PassSpec make_pass(const Schedule& s, int vi, long long batch, long long 
   return p;
 }
 
+// Switch a pass to its specialised kernel when pac_special.h has one for its
+// geometry and the tile fits the lines (W divides nlines and the stride).
+static void apply_special(const Schedule& s, PassSpec& p) {
+  PassDesc& d = p.d;
+  int logW = 0, nt = 0;
+  if (d.nat) return;
+  if (!special_geometry(s.bytes, s.b2, d.mode, d.sign, d.logL, d.logS > 0 ? 1 : 0, &logW, &nt))
+    return;
+  const long long W = 1LL << logW;
+  if ((d.nlines & (W - 1)) != 0) return;
+  if (d.logS > 0 && logW > d.logS) return;
+  d.W = (int)W;
+  d.logW = logW;
+  d.pitch = pitch_for(s.bytes, d.logL, d.W);
+  d.nthreads = nt;
+  d.spec = 1;
+  p.threads = nt;
+  p.grid = d.nlines / W;
+  p.smem = (size_t)2 * d.W * d.pitch * s.bytes;
+}
+
 static int launch(const Schedule& s, PassSpec& p, void* stream) {
   return be_launch_pass(p.d, s.bytes, s.b2, p.grid, p.threads, p.smem, stream);
 }
@@ -313,6 +315,7 @@ static int launch(const Schedule& s, PassSpec& p, void* stream) {
 // events and accumulate the per-pass milliseconds in the plan.
 static int exec_passes(pac_plan_s* pl, const Schedule& s, std::vector<PassSpec>& passes,
                        void* stream) {
+  for (auto& p : passes) apply_special(s, p);
   if (!pl->timing) {
     for (auto& p : passes) PAC_TRY(launch(s, p, stream));
     return PAC_SUCCESS;

@@ -1,0 +1,480 @@
+// pac_stages.cuh -- butterfly stages and pass bodies of the engine.
+//
+// One radix-R butterfly of a stage:
+//   DIF: load x[m] @ j + ell*m, DFT, twiddle output s by w_K^{j s},
+//        store @ j + ell*sigma_b(s)
+//   DIT: load x[s] @ j + ell*sigma_b(s), twiddle by w_K^{j s}, DFT,
+//        store @ j + ell*m
+// Global-facing stages read (first) or write (last) the line in global
+// memory; all other accesses go to the padded shared-memory line.
+//
+// The same stage code serves two kinds of kernels through a shape policy:
+// the generic kernel reads every geometry value (line length, tile width,
+// pitch, stride kind) from the PassDesc at run time; a specialised kernel
+// fixes them at compile time together with its radix schedule, so the index
+// arithmetic folds into constants.
+#pragma once
+
+namespace pac {
+
+enum { IO_SMEM = 0, IO_GLOBAL = 1 };
+
+// geometry policy; -1 = read from the PassDesc at run time
+template <int LOGL_ = -1, int LOGW_ = -1, int PITCH_ = -1, int COLS_ = -1>
+struct Shape {
+  static constexpr int kLogL = LOGL_;
+  static constexpr int kLogW = LOGW_;
+  static constexpr int kPitch = PITCH_;
+  static constexpr int kCols = COLS_;
+  static PAC_HD int logL(const PassDesc& d) {
+    if constexpr (LOGL_ >= 0) return LOGL_;
+    else return d.logL;
+  }
+  static PAC_HD int logW(const PassDesc& d) {
+    if constexpr (LOGW_ >= 0) return LOGW_;
+    else return d.logW;
+  }
+  static PAC_HD int W(const PassDesc& d) { return 1 << logW(d); }
+  static PAC_HD int pitch(const PassDesc& d) {
+    if constexpr (PITCH_ >= 0) return PITCH_;
+    else return d.pitch;
+  }
+  // lines of the tile are consecutive columns (element stride S > 1)
+  static PAC_HD bool cols(const PassDesc& d) {
+    if constexpr (COLS_ >= 0) return COLS_ != 0;
+    else return d.logS > 0;
+  }
+};
+using RtShape = Shape<>;
+
+// butterfly index -> (w, blk, j) for a stage of block 2^logK, radix 2^logR
+template <class SP>
+PAC_HD void bf_coords(const PassDesc& d, int logK, int logR, bool global_facing, int u, int* w,
+                      int* blk, int* j) {
+  const int lbf = SP::logL(d) - logR;  // butterflies per line (log)
+  const int logell = logK - logR;
+  int v;
+  if (global_facing && SP::cols(d)) {
+    // consecutive threads take consecutive columns: coalesced rows of W
+    *w = u & (SP::W(d) - 1);
+    v = u >> SP::logW(d);
+  } else {
+    v = u & ((1 << lbf) - 1);
+    *w = u >> lbf;
+  }
+  *blk = v >> logell;
+  *j = v & ((1 << logell) - 1);
+}
+
+// The 4-step twiddle w_N^{iG * rev_b(e)} of line w at element e.
+template <typename T, int B2, class SP>
+PAC_HD Cx<T> tw4_value(const PassDesc& d, long long cta, int w, int e) {
+  long long g = cta * SP::W(d) + w;
+  long long i = g & ((1LL << d.logS) - 1);
+  uint32_t iG = (uint32_t)((i >> d.tw4_shift) & d.tw4_mask);
+  uint32_t E = iG * drev<B2>((uint32_t)e, SP::logL(d));
+  const Cx<T>* lo = (const Cx<T>*)d.tw4_lo;
+  const Cx<T>* hi = (const Cx<T>*)d.tw4_hi;
+  return cmul(ld_tw(lo + (E & ((1u << d.tw4_lolog) - 1))), ld_tw(hi + (E >> d.tw4_lolog)));
+}
+
+// One butterfly.  CLOGK >= 0 fixes the stage's block size at compile time.
+template <typename T, int B2, int R, int SIGN, bool DIF, class SP, int CLOGK>
+PAC_HD void stage_bf(const PassDesc& d, long long cta, T* sre, T* sim, int logK_rt, int twoff,
+                     int src, int dst, int u, const long long* lbase_in,
+                     const long long* lbase_out) {
+  constexpr int LR = ilog2(R);
+  static_assert(LR % B2 == 0, "radix must be a power of the digit base");
+  const int logK = CLOGK >= 0 ? CLOGK : logK_rt;
+  const int logell = logK - LR;
+  int w, blk, j;
+  bf_coords<SP>(d, logK, LR, src == IO_GLOBAL || dst == IO_GLOBAL, u, &w, &blk, &j);
+  const int ell = 1 << logell;
+  const int e0 = (blk << logK) + j;
+  const int pitch = SP::pitch(d);
+  const T* ire = (const T*)d.in_re;
+  const T* iim = (const T*)d.in_im;
+  Cx<T> x[R];
+  // ---- load
+  static_for<R>([&](auto mm) {
+    constexpr int m = mm.value;
+    constexpr int slot = DIF ? m : drev_c(m, LR, B2);
+    const int e = e0 + ell * slot;
+    if (src == IO_GLOBAL) {
+      long long gi = lbase_in[w] + ((long long)e << d.logS);
+      x[m] = Cx<T>{ld_g(ire + gi), ld_g(iim + gi)};
+    } else {
+      int si = w * pitch + sidx<T>(e);
+      x[m] = Cx<T>{sre[si], sim[si]};
+    }
+  });
+  const Cx<T>* tw = (const Cx<T>*)d.tw + twoff + j * (R - 1);
+  const bool twiddle = logell > 0 && j > 0;
+  if constexpr (!DIF) {
+    // 4-step pre-twiddle: only the innermost stage (ell == 1) of a DIT pass
+    if (d.tw4 == 2 && logell == 0) {
+      static_for<R>([&](auto mm) {
+        constexpr int slot = drev_c(mm.value, LR, B2);
+        x[mm.value] = ctw(x[mm.value], tw4_value<T, B2, SP>(d, cta, w, e0 + slot), SIGN);
+      });
+    }
+    if (twiddle) {
+      static_for<R - 1>([&](auto ss) {
+        constexpr int s = ss.value + 1;
+        x[s] = ctw(x[s], ld_tw(tw + (s - 1)), SIGN);
+      });
+    }
+  }
+  dft_reg<T, R, SIGN>(x);
+  // register p now holds output index brev(p)
+  if constexpr (DIF) {
+    if (twiddle) {
+      static_for<R>([&](auto pp) {
+        constexpr int s = brev_c(pp.value, LR);
+        if constexpr (s > 0) x[pp.value] = ctw(x[pp.value], ld_tw(tw + (s - 1)), SIGN);
+      });
+    }
+    // 4-step post-twiddle: only the innermost stage of a DIF pass
+    if (d.tw4 == 1 && logell == 0) {
+      static_for<R>([&](auto pp) {
+        constexpr int slot = drev_c(brev_c(pp.value, LR), LR, B2);
+        x[pp.value] = ctw(x[pp.value], tw4_value<T, B2, SP>(d, cta, w, e0 + slot), SIGN);
+      });
+    }
+  }
+  // ---- store
+  T* ore = (T*)d.out_re;
+  T* oim = (T*)d.out_im;
+  static_for<R>([&](auto pp) {
+    constexpr int p = pp.value;
+    constexpr int slot = DIF ? drev_c(brev_c(p, LR), LR, B2) : brev_c(p, LR);
+    const int e = e0 + ell * slot;
+    Cx<T> v = x[p];
+    if (dst == IO_GLOBAL) {
+      if (d.use_scale) {
+        v.re *= T(d.scale);
+        v.im *= T(d.scale);
+      }
+      long long gi = lbase_out[w] + ((long long)e << d.logS);
+      ore[gi] = v.re;
+      oim[gi] = v.im;
+    } else {
+      int si = w * pitch + sidx<T>(e);
+      sre[si] = v.re;
+      sim[si] = v.im;
+    }
+  });
+}
+
+// Convolution middle: the last DIF stage (ell == 1), the pointwise product
+// with the filter spectrum at the same P_b positions, and the first DIT
+// stage, all in registers.
+template <typename T, int B2, int R, class SP>
+PAC_HD void middle_bf(const PassDesc& d, T* sre, T* sim, int src, int dst, int u,
+                      const long long* lbase) {
+  constexpr int LR = ilog2(R);
+  int w, blk, j;
+  bf_coords<SP>(d, LR, LR, src == IO_GLOBAL || dst == IO_GLOBAL, u, &w, &blk, &j);
+  const int e0 = blk << LR;  // ell == 1, j == 0
+  const int pitch = SP::pitch(d);
+  const T* ire = (const T*)d.in_re;
+  const T* iim = (const T*)d.in_im;
+  const T* hre = (const T*)d.h_re;
+  const T* him = (const T*)d.h_im;
+  Cx<T> x[R];
+  static_for<R>([&](auto mm) {
+    constexpr int m = mm.value;
+    const int e = e0 + m;
+    if (src == IO_GLOBAL) {
+      long long gi = lbase[w] + ((long long)e << d.logS);
+      x[m] = Cx<T>{ld_g(ire + gi), ld_g(iim + gi)};
+    } else {
+      int si = w * pitch + sidx<T>(e);
+      x[m] = Cx<T>{sre[si], sim[si]};
+    }
+  });
+  dft_reg<T, R, -1>(x);
+  // register p holds the spectrum at slot sigma_b(brev(p)); the DIT stage
+  // wants register s = the value at slot sigma_b(s), i.e. register brev(s).
+  Cx<T> y[R];
+  const T sc = T(d.scale);
+  static_for<R>([&](auto ss) {
+    constexpr int s = ss.value;
+    constexpr int p = brev_c(s, LR);
+    const int e = e0 + drev_c(s, LR, B2);
+    long long hi = (lbase[w] + ((long long)e << d.logS)) & d.h_mask;
+    Cx<T> hv = Cx<T>{ld_g(hre + hi) * sc, ld_g(him + hi) * sc};
+    y[s] = cmul(x[p], hv);
+  });
+  dft_reg<T, R, +1>(y);
+  T* ore = (T*)d.out_re;
+  T* oim = (T*)d.out_im;
+  static_for<R>([&](auto pp) {
+    constexpr int p = pp.value;
+    const int e = e0 + brev_c(p, LR);
+    if (dst == IO_GLOBAL) {
+      long long gi = lbase[w] + ((long long)e << d.logS);
+      ore[gi] = y[p].re;
+      oim[gi] = y[p].im;
+    } else {
+      int si = w * pitch + sidx<T>(e);
+      sre[si] = y[p].re;
+      sim[si] = y[p].im;
+    }
+  });
+}
+
+// ---------------------------------------------------------------------------
+// Phases: a loop over butterflies; the device runs it with one butterfly per
+// thread, the host emulator with a plain loop.  Barriers separate a phase
+// that writes shared memory from the next phase that reads it.
+// ---------------------------------------------------------------------------
+#if defined(__CUDA_ARCH__)
+#define PAC_FOR_BF(n, u) for (int u = (int)threadIdx.x; u < (n); u += (int)blockDim.x)
+#define PAC_SYNC() __syncthreads()
+#else
+#define PAC_FOR_BF(n, u) for (int u = 0; u < (n); ++u)
+#define PAC_SYNC() ((void)0)
+#endif
+
+// ---------------------------------------------------------------------------
+// Generic pass body: geometry and radix schedule at run time
+// ---------------------------------------------------------------------------
+template <typename T, int B2, bool DIF>
+PAC_HD void stage_dispatch(const PassDesc& d, long long cta, T* sre, T* sim, int logK, int logR,
+                           int twoff, int sign, int src, int dst, int u, const long long* lbi,
+                           const long long* lbo) {
+#define PAC_ST(RR)                                                                     \
+  if (sign < 0)                                                                        \
+    stage_bf<T, B2, RR, -1, DIF, RtShape, -1>(d, cta, sre, sim, logK, twoff, src, dst, u, \
+                                              lbi, lbo);                               \
+  else                                                                                 \
+    stage_bf<T, B2, RR, +1, DIF, RtShape, -1>(d, cta, sre, sim, logK, twoff, src, dst, u, \
+                                              lbi, lbo);
+  if constexpr (B2 == 1) {
+    switch (logR) {
+      case 1: PAC_ST(2) break;
+      case 2: PAC_ST(4) break;
+      case 3: PAC_ST(8) break;
+      default: PAC_ST(16) break;
+    }
+  } else if constexpr (B2 == 2) {
+    if (logR == 2) {
+      PAC_ST(4)
+    } else {
+      PAC_ST(16)
+    }
+  } else {
+    PAC_ST(8)
+  }
+#undef PAC_ST
+}
+
+template <typename T, int B2>
+PAC_HD void middle_dispatch(const PassDesc& d, T* sre, T* sim, int logR, int src, int dst, int u,
+                            const long long* lb) {
+  if constexpr (B2 == 1) {
+    switch (logR) {
+      case 1: middle_bf<T, B2, 2, RtShape>(d, sre, sim, src, dst, u, lb); break;
+      case 2: middle_bf<T, B2, 4, RtShape>(d, sre, sim, src, dst, u, lb); break;
+      case 3: middle_bf<T, B2, 8, RtShape>(d, sre, sim, src, dst, u, lb); break;
+      default: middle_bf<T, B2, 16, RtShape>(d, sre, sim, src, dst, u, lb); break;
+    }
+  } else if constexpr (B2 == 2) {
+    if (logR == 2) middle_bf<T, B2, 4, RtShape>(d, sre, sim, src, dst, u, lb);
+    else middle_bf<T, B2, 16, RtShape>(d, sre, sim, src, dst, u, lb);
+  } else {
+    middle_bf<T, B2, 8, RtShape>(d, sre, sim, src, dst, u, lb);
+  }
+}
+
+// block size (log) of stage i of the DIF order: L / (R_0 ... R_{i-1})
+PAC_HD int stage_logK(const PassDesc& d, int i) {
+  int logK = d.logL;
+  for (int q = 0; q < i; ++q) logK -= d.rlog[q];
+  return logK;
+}
+
+template <typename T, int B2>
+PAC_HD void pass_body(const PassDesc& d, long long cta, T* sre, T* sim, const long long* lbi,
+                      const long long* lbo) {
+  const bool nat = d.nat != 0;
+  const int nst = d.nst;
+  if (d.mode == MODE_DIF) {
+    for (int i = 0; i < nst; ++i) {
+      int logK = stage_logK(d, i), logR = d.rlog[i];
+      int src = (i == 0) ? IO_GLOBAL : IO_SMEM;
+      int dst = (i == nst - 1 && !nat) ? IO_GLOBAL : IO_SMEM;
+      int nbf = d.W << (d.logL - logR);
+      if (i > 0) PAC_SYNC();
+      PAC_FOR_BF(nbf, u) {
+        stage_dispatch<T, B2, true>(d, cta, sre, sim, logK, logR, d.tw_off[i], d.sign, src, dst, u,
+                                    lbi, lbo);
+      }
+    }
+    if (nat) {
+      // natural-order store out of shared memory
+      PAC_SYNC();
+      T* ore = (T*)d.out_re;
+      T* oim = (T*)d.out_im;
+      const int n = d.W << d.logL;
+      const bool lines_fast = d.logS > 0 || d.nat_nf > 0;
+      PAC_FOR_BF(n, u) {
+        int w, q;
+        if (lines_fast) {
+          w = u & (d.W - 1);
+          q = u >> d.logW;
+        } else {
+          w = u >> d.logL;
+          q = u & (d.L - 1);
+        }
+        // q is the natural index inside this factor: it sits at slot rev(q)
+        int e = (int)drev<B2>((uint32_t)q, d.logL);
+        int si = w * d.pitch + sidx<T>(e);
+        T vr = sre[si], vi = sim[si];
+        if (d.use_scale) {
+          vr *= T(d.scale);
+          vi *= T(d.scale);
+        }
+        long long gi = lbo[w] + ((long long)q << (d.nat_Mlog + d.logS));
+        ore[gi] = vr;
+        oim[gi] = vi;
+      }
+    }
+  } else if (d.mode == MODE_DIT) {
+    for (int k = 0; k < nst; ++k) {
+      int i = nst - 1 - k;
+      int logK = stage_logK(d, i), logR = d.rlog[i];
+      int src = (k == 0) ? IO_GLOBAL : IO_SMEM;
+      int dst = (k == nst - 1) ? IO_GLOBAL : IO_SMEM;
+      int nbf = d.W << (d.logL - logR);
+      if (k > 0) PAC_SYNC();
+      PAC_FOR_BF(nbf, u) {
+        stage_dispatch<T, B2, false>(d, cta, sre, sim, logK, logR, d.tw_off[i], d.sign, src, dst,
+                                     u, lbi, lbo);
+      }
+    }
+  } else {  // MODE_CONV
+    for (int i = 0; i < nst - 1; ++i) {
+      int logK = stage_logK(d, i), logR = d.rlog[i];
+      int src = (i == 0) ? IO_GLOBAL : IO_SMEM;
+      int nbf = d.W << (d.logL - logR);
+      if (i > 0) PAC_SYNC();
+      PAC_FOR_BF(nbf, u) {
+        stage_dispatch<T, B2, true>(d, cta, sre, sim, logK, logR, d.tw_off[i], -1, src, IO_SMEM,
+                                    u, lbi, lbo);
+      }
+    }
+    {
+      int logR = d.rlog[nst - 1];
+      int src = (nst == 1) ? IO_GLOBAL : IO_SMEM;
+      int dst = (nst == 1) ? IO_GLOBAL : IO_SMEM;
+      int nbf = d.W << (d.logL - logR);
+      if (nst > 1) PAC_SYNC();
+      PAC_FOR_BF(nbf, u) { middle_dispatch<T, B2>(d, sre, sim, logR, src, dst, u, lbi); }
+    }
+    for (int i = nst - 2; i >= 0; --i) {
+      int logK = stage_logK(d, i), logR = d.rlog[i];
+      int dst = (i == 0) ? IO_GLOBAL : IO_SMEM;
+      int nbf = d.W << (d.logL - logR);
+      PAC_SYNC();
+      PAC_FOR_BF(nbf, u) {
+        stage_dispatch<T, B2, false>(d, cta, sre, sim, logK, logR, d.tw_off[i], +1, IO_SMEM, dst,
+                                     u, lbi, lbo);
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Specialised pass body: shape and radix schedule fixed at compile time
+// (RL = radix logs in DIF order, outermost first).  DIF, DIT and CONV.
+// ---------------------------------------------------------------------------
+template <int... RL>
+struct Rads {
+  static constexpr int n = sizeof...(RL);
+  static constexpr int v[n] = {RL...};
+  // block size (log) of stage i
+  static PAC_HDC int logK(int logL, int i) {
+    int k = logL;
+    for (int q = 0; q < i; ++q) k -= v[q];
+    return k;
+  }
+};
+
+#if defined(__CUDA_ARCH__)
+#define PAC_FOR_BF_CT(n, NT, u)                                        \
+  _Pragma("unroll") for (int u##_base = 0; u##_base < (n); u##_base += (NT)) \
+    for (int u = u##_base + (int)threadIdx.x; u < u##_base + (NT) && u < (n); u += (NT))
+#else
+#define PAC_FOR_BF_CT(n, NT, u) for (int u = 0; u < (n); ++u)
+#endif
+
+template <typename T, int B2, int MODE, int SIGN, class SP, int NT, class RS>
+PAC_HD void pass_body_ct(const PassDesc& d, long long cta, T* sre, T* sim, const long long* lbi,
+                         const long long* lbo) {
+  constexpr int LOGL = SP::kLogL;
+  constexpr int LOGW = SP::kLogW;
+  static_assert(LOGL >= 0 && LOGW >= 0 && SP::kPitch >= 0 && SP::kCols >= 0, "fixed shape");
+  constexpr int n = RS::n;
+  if constexpr (MODE == MODE_DIF) {
+    static_for<n>([&](auto ii) {
+      constexpr int i = ii.value;
+      constexpr int LK = RS::logK(LOGL, i);
+      constexpr int LRr = RS::v[i];
+      constexpr int nbf = 1 << (LOGW + LOGL - LRr);
+      if constexpr (i > 0) PAC_SYNC();
+      PAC_FOR_BF_CT(nbf, NT, u) {
+        stage_bf<T, B2, (1 << LRr), SIGN, true, SP, LK>(
+            d, cta, sre, sim, LK, d.tw_off[i], i == 0 ? IO_GLOBAL : IO_SMEM,
+            i == n - 1 ? IO_GLOBAL : IO_SMEM, u, lbi, lbo);
+      }
+    });
+  } else if constexpr (MODE == MODE_DIT) {
+    static_for<n>([&](auto kk) {
+      constexpr int k = kk.value;
+      constexpr int i = n - 1 - k;
+      constexpr int LK = RS::logK(LOGL, i);
+      constexpr int LRr = RS::v[i];
+      constexpr int nbf = 1 << (LOGW + LOGL - LRr);
+      if constexpr (k > 0) PAC_SYNC();
+      PAC_FOR_BF_CT(nbf, NT, u) {
+        stage_bf<T, B2, (1 << LRr), SIGN, false, SP, LK>(
+            d, cta, sre, sim, LK, d.tw_off[i], k == 0 ? IO_GLOBAL : IO_SMEM,
+            k == n - 1 ? IO_GLOBAL : IO_SMEM, u, lbi, lbo);
+      }
+    });
+  } else {
+    static_for<n - 1>([&](auto ii) {
+      constexpr int i = ii.value;
+      constexpr int LK = RS::logK(LOGL, i);
+      constexpr int LRr = RS::v[i];
+      constexpr int nbf = 1 << (LOGW + LOGL - LRr);
+      if constexpr (i > 0) PAC_SYNC();
+      PAC_FOR_BF_CT(nbf, NT, u) {
+        stage_bf<T, B2, (1 << LRr), -1, true, SP, LK>(
+            d, cta, sre, sim, LK, d.tw_off[i], i == 0 ? IO_GLOBAL : IO_SMEM, IO_SMEM, u, lbi, lbo);
+      }
+    });
+    {
+      constexpr int LRr = RS::v[n - 1];
+      constexpr int nbf = 1 << (LOGW + LOGL - LRr);
+      constexpr int io = n == 1 ? IO_GLOBAL : IO_SMEM;
+      if constexpr (n > 1) PAC_SYNC();
+      PAC_FOR_BF_CT(nbf, NT, u) { middle_bf<T, B2, (1 << LRr), SP>(d, sre, sim, io, io, u, lbi); }
+    }
+    static_for<n - 1>([&](auto kk) {
+      constexpr int i = n - 2 - kk.value;
+      constexpr int LK = RS::logK(LOGL, i);
+      constexpr int LRr = RS::v[i];
+      constexpr int nbf = 1 << (LOGW + LOGL - LRr);
+      PAC_SYNC();
+      PAC_FOR_BF_CT(nbf, NT, u) {
+        stage_bf<T, B2, (1 << LRr), +1, false, SP, LK>(
+            d, cta, sre, sim, LK, d.tw_off[i], IO_SMEM, i == 0 ? IO_GLOBAL : IO_SMEM, u, lbi, lbo);
+      }
+    });
+  }
+}
+
+}  // namespace pac

@@ -37,7 +37,10 @@ def test_multi_factor_splits(emu, orc, cap, monkeypatch):
 @pytest.mark.parametrize("dims,batch,base,form,per", [
     ((1024,), 4, 2, 0, False), ((4 ** 7,), 2, 4, 0, True), ((64, 32), 3, 2, 1, False),
     ((2 ** 14,), 2, 2, 1, True), ((16, 16, 16), 2, 4, 1, False), ((8 ** 3,), 2, 8, 0, False), ((1024,), 5, 2, 0, False),
-    ((256,), 3, 4, 1, True), ((4096,), 7, 4, 0, False)])
+    ((256,), 3, 4, 1, True), ((4096,), 7, 4, 0, False),
+    # geometries served by the specialised kernels (pac_special.h)
+    ((2048, 64), 1, 2, 0, False), ((64, 2048), 2, 2, 0, False), ((2048, 32), 1, 2, 1, False),
+    ((32, 2048), 2, 2, 1, True)])
 def test_native_conv(emu, dims, batch, base, form, per):
     g = rng(21)
     shape = (batch,) + dims

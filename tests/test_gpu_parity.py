@@ -120,6 +120,8 @@ def test_c4_3d_f64_against_oracle(lib, orc):
     ((1024,), 4, 2, 0, False), ((4 ** 7,), 2, 4, 0, True), ((64, 32), 3, 2, 1, False),
     ((2 ** 14,), 2, 2, 1, True), ((16, 16, 16), 2, 4, 1, False), ((8 ** 3,), 2, 8, 0, False), ((1024,), 5, 2, 0, False),
     ((256,), 3, 4, 1, True), ((4096,), 7, 4, 0, False),
+    ((2048, 64), 1, 2, 0, False), ((64, 2048), 2, 2, 0, False), ((2048, 32), 1, 2, 1, False),
+    ((32, 2048), 2, 2, 1, True),
     ((2 ** 20,), 2, 2, 0, False), ((2 ** 20,), 2, 2, 1, False)])
 def test_native_conv(lib, dims, batch, base, form, per):
     g = rng(21)
