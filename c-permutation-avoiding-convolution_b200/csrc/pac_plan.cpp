@@ -169,7 +169,9 @@ static int build_schedule(Schedule& s, int rank, const int* logs, int b2, int by
     PAC_TRY(be_fill_pow_tw(t.hi, bytes, nhi, nlo, logN, nullptr));
     s.tw4[logN] = t;
   }
-  return PAC_SUCCESS;
+  // the tables are filled on the legacy stream, which does not order against
+  // non-blocking streams: finish them before the plan is handed out
+  return be_stream_sync(nullptr);
 }
 
 }  // namespace pac
