@@ -64,6 +64,8 @@ def _declare(L):
     L.pac_filter_spectrum.argtypes = [_vp, _vp, _vp, i, _vp, _vp, d, _vp]
     L.pac_convolve.argtypes = [_vp, _vp, _vp, _vp, _vp, i, _vp, _vp, d, _vp]
     L.pac_transform.argtypes = [_vp, i, _vp, _vp, _vp, _vp, _vp]
+    if hasattr(L, "pac_convolve_1d_noalloc"):  # product library only
+        L.pac_convolve_1d_noalloc.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, i, i, _vp]
     L.pac_pointwise_product.argtypes = [ll, _vp, _vp, _vp, _vp, _vp, _vp, d, _vp]
     L.pac_scale.argtypes = [ll, _vp, _vp, _vp, _vp, d, _vp]
     L.pac_permute.argtypes = [ll, _vp, _vp, _vp, _vp]

@@ -491,6 +491,103 @@ static int run_conv(pac_plan_s* pl, const void* x_re, const void* x_im, const vo
   return exec_passes(pl, s, passes, stream);
 }
 
+// ---------------------------------------------------------------------------
+// 1D convolution in caller-supplied device scratch (pac_convolve_1d_noalloc).
+// The twiddle tables and the filter spectrum are carved out of `scratch` in
+// 256-byte aligned pieces and regenerated on `stream` by every call, so a
+// call never depends on what an earlier call left there.  Nothing here
+// allocates device memory.
+// ---------------------------------------------------------------------------
+struct Arena {
+  char* cur;
+  char* end;
+  void* take(size_t bytes) {
+    size_t a = (bytes + 255) & ~(size_t)255;
+    if (cur + a > end) return nullptr;
+    void* p = cur;
+    cur += a;
+    return p;
+  }
+};
+
+static int build_schedule_in_arena(Schedule& s, int logn, Arena& ar, void* stream) {
+  s.bytes = 8;
+  s.b2 = 1;
+  const int lmax = max_factor_log(8, 1);
+  if (logn > 0) {
+    int nf = (logn + lmax - 1) / lmax;
+    if (nf > PAC_MAX_FACTORS) return set_error(PAC_ERROR_SIZE, "too many factors");
+    std::vector<int> parts(nf, logn / nf);
+    for (int i = 0; i < logn % nf; ++i) parts[nf - 1 - i]++;
+    for (int f = 0; f < nf; ++f) s.vax.push_back({parts[f], 0, f == 0, f == nf - 1});
+  }
+  for (auto& v : s.vax) s.rad.push_back(radix_schedule(v.log, 1));
+  long long total = 0;
+  std::vector<std::pair<int, int>> specs;
+  for (size_t i = 0; i < s.vax.size(); ++i) {
+    int logK = s.vax[i].log;
+    for (int rl : s.rad[i]) {
+      std::pair<int, int> key(logK, rl);
+      if (!s.tw_off.count(key) && logK > rl) {
+        s.tw_off[key] = (int)total;
+        specs.push_back(key);
+        total += (1LL << (logK - rl)) * ((1LL << rl) - 1);
+      }
+      logK -= rl;
+    }
+  }
+  if (total > 0) {
+    s.pool = ar.take((size_t)total * 16);
+    if (!s.pool) return set_error(PAC_ERROR_SIZE, "no-allocation scratch too small");
+    for (auto& k : specs)
+      PAC_TRY(be_fill_stage_tw((char*)s.pool + (size_t)s.tw_off[k] * 16, 8, k.first, k.second,
+                               stream));
+  }
+  for (size_t i = 0; i < s.vax.size(); ++i) {
+    if (s.vax[i].last) continue;
+    int logN = 0;
+    for (size_t j = i; j < s.vax.size(); ++j) logN += s.vax[j].log;
+    if (s.tw4.count(logN)) continue;
+    Schedule::Tw4 t;
+    t.lolog = (logN + 1) / 2;
+    long long nlo = 1LL << t.lolog, nhi = 1LL << (logN - t.lolog);
+    t.lo = ar.take((size_t)nlo * 16);
+    t.hi = ar.take((size_t)nhi * 16);
+    if (!t.lo || !t.hi) return set_error(PAC_ERROR_SIZE, "no-allocation scratch too small");
+    s.tw4[logN] = t;
+    PAC_TRY(be_fill_pow_tw(t.lo, 8, nlo, 1, logN, stream));
+    PAC_TRY(be_fill_pow_tw(t.hi, 8, nhi, nlo, logN, stream));
+  }
+  return PAC_SUCCESS;
+}
+
+int conv_in_scratch(void* scratch, size_t scratch_bytes, int logn, int batch, const double* x_re,
+                    const double* x_im, const double* h_re, const double* h_im, double* y_re,
+                    double* y_im, void* stream) {
+  pac_plan_s pl;
+  pl.rank = 1;
+  pl.dims[0] = 1 << logn;
+  pl.logs[0] = logn;
+  pl.batch = batch;
+  pl.b2 = 1;
+  pl.form = PAC_FORM_F64;
+  pl.N = 1LL << logn;
+  Arena ar{(char*)scratch, (char*)scratch + scratch_bytes};
+  int st = build_schedule_in_arena(pl.main, logn, ar, stream);
+  double* hre = (double*)ar.take((size_t)pl.N * 8);
+  double* him = (double*)ar.take((size_t)pl.N * 8);
+  if (st == PAC_SUCCESS && (!hre || !him))
+    st = set_error(PAC_ERROR_SIZE, "no-allocation scratch too small");
+  if (st == PAC_SUCCESS)
+    st = run_transform(&pl, pl.main, PAC_OP_AT, 1, h_re, h_im, hre, him, 1.0 / (double)pl.N, 1,
+                       stream);
+  if (st == PAC_SUCCESS) st = run_conv(&pl, x_re, x_im, hre, him, 0, y_re, y_im, 1.0, stream);
+  // the tables live in the caller's scratch: nothing to free
+  pl.main.pool = nullptr;
+  pl.main.tw4.clear();
+  return st;
+}
+
 }  // namespace pac
 
 // ---------------------------------------------------------------------------

@@ -124,6 +124,24 @@ PAC_API int pac_convolve(pac_plan_t plan, const void* x_re, const void* x_im,
 PAC_API int pac_transform(pac_plan_t plan, int op, const void* in_re, const void* in_im,
                           void* out_re, void* out_im, pac_stream_t stream);
 
+/* No counterpart in the reference.  Circular convolution of each of `batch`
+ * complex FP64 signals of length n (a power of 2, at most
+ * PAC_NOALLOC_MAX_N) with one filter h, for callers that cannot allocate
+ * device memory (inside another framework's memory pool, under a fixed
+ * memory budget, or where an allocation could synchronise the device).
+ * x, h and y are device arrays the caller owns (x may alias y; x is
+ * batch * n elements, h is n).  The call allocates nothing: its twiddle
+ * tables and filter spectrum live in a fixed static device array of this
+ * library, held by every GPU that loads it until the process exits.  The
+ * first call on a device looks up that array's address once.  Calls whose
+ * device work overlaps (other streams or host threads) race on the shared
+ * array; queue them on one stream.  n above the limit returns
+ * PAC_ERROR_SIZE and leaves y untouched. */
+#define PAC_NOALLOC_MAX_N 65536
+PAC_API int pac_convolve_1d_noalloc(const double* x_re, const double* x_im, const double* h_re,
+                                    const double* h_im, double* y_re, double* y_im, int n,
+                                    int batch, pac_stream_t stream);
+
 /* y = scale * x .* h elementwise over n complex FP64 values (the product
  * loop of convolution.c:55-62 on its own; the reference's convolution
  * reduces to it when the radix is not supported). */
