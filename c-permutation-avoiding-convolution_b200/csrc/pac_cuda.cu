@@ -9,6 +9,7 @@
 //
 // There is no host fallback: every entry point requires an sm_100 device and
 // fails with PAC_ERROR_NO_DEVICE otherwise.
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 #include <stdio.h>
 
@@ -34,6 +35,11 @@ static int cuda_fail(cudaError_t e, const char* what) {
   do {                                          \
     cudaError_t _e = (call);                    \
     if (_e != cudaSuccess) return cuda_fail(_e, what); \
+  } while (0)
+#define PAC_TRY_BE(expr)                 \
+  do {                                   \
+    int _st = (expr);                    \
+    if (_st != PAC_SUCCESS) return _st;  \
   } while (0)
 
 // ---------------------------------------------------------------------------
@@ -77,13 +83,130 @@ __global__ void __launch_bounds__(NT, MINB) pac_special_kernel(const PassDesc d)
   pass_body_ct<T, B2, MODE, SIGN, SP, NT, RadsFor<LOGL, B2>>(d, cta, sre, sim, s_lb, s_lb);
 }
 
+// ---------------------------------------------------------------------------
+// TMA column passes
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void fence_barrier_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded: gives up after ~2^32 SM cycles (about 2 s) instead of spinning forever
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity)) {
+    if (clock64() - t0 > (1LL << 32)) return false;
+  }
+  return true;
+}
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0,
+                                            int c1, int c2) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
+      "l"((uint64_t)map), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, const void* src, int c0, int c1,
+                                             int c2) {
+  asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(
+                   (uint64_t)map),
+               "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(src))
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() {
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_wait_read0() {
+  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// A column pass (DIF or DIT) over a tile of W columns x L rows that TMA
+// copies into shared memory and back: one elected thread issues the tensor
+// copies, everyone waits on an mbarrier (bounded), the stages run on the
+// swizzled tile, and the tile is stored by tensor copies.
+template <typename T, int B2, int MODE, int SIGN, int LOGL, int LOGW, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB)
+    pac_tma_col_kernel(const PassDesc d, const __grid_constant__ CUtensorMap tin_re,
+                       const __grid_constant__ CUtensorMap tin_im,
+                       const __grid_constant__ CUtensorMap tout_re,
+                       const __grid_constant__ CUtensorMap tout_im) {
+  constexpr int W = 1 << LOGW, L = 1 << LOGL;
+  constexpr int BOXR = tma_boxr(LOGL), NBOX = L / BOXR;
+  static_assert(W * sizeof(T) == 16, "16-byte tensor rows");
+  using SP = TmaShape<LOGL, LOGW, (int)sizeof(T)>;
+  extern __shared__ unsigned char pac_smem_raw[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ long long s_lb[W];
+  T* sre = reinterpret_cast<T*>(((uintptr_t)pac_smem_raw + 1023) & ~(uintptr_t)1023);
+  T* sim = sre + (size_t)W * L;
+  const long long cta = blockIdx.x;
+  const long long g0 = cta * W;
+  const int i0 = (int)(g0 & ((1LL << d.logS) - 1));
+  const int o = (int)(g0 >> d.logS);
+  if ((int)threadIdx.x < W) s_lb[threadIdx.x] = line_base(d, g0 + threadIdx.x);
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    mbar_arrive_expect_tx(&bar, (uint32_t)(2 * W * L * sizeof(T)));
+    for (int k = 0; k < NBOX; ++k) {
+      tma_load_3d(sre + (size_t)k * BOXR * W, &tin_re, &bar, i0, k * BOXR, o);
+      tma_load_3d(sim + (size_t)k * BOXR * W, &tin_im, &bar, i0, k * BOXR, o);
+    }
+  }
+  if (!mbar_wait_bounded(&bar, 0)) {
+    if (threadIdx.x == 0 && d.status) atomicExch(d.status, PAC_ERROR_TIMEOUT);
+    return;
+  }
+  pass_body_ct<T, B2, MODE, SIGN, SP, NT, RadsFor<LOGL, B2>, true>(d, cta, sre, sim, s_lb, s_lb);
+  // generic-proxy writes of the tile become visible to the tensor copy
+  fence_proxy_async();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < NBOX; ++k) {
+      tma_store_3d(&tout_re, sre + (size_t)k * BOXR * W, i0, k * BOXR, o);
+      tma_store_3d(&tout_im, sim + (size_t)k * BOXR * W, i0, k * BOXR, o);
+    }
+    bulk_commit();
+    bulk_wait_read0();  // the tile must outlive the copies that read it
+  }
+}
+
 template <typename T>
 __global__ void fill_stage_tw_kernel(Cx<T>* dst, int logK, int logR) {
   const long long R1 = (1LL << logR) - 1;
   const long long n = (1LL << (logK - logR)) * R1;
   for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < n;
        idx += (long long)gridDim.x * blockDim.x) {
-    long long j = idx / R1, s = idx % R1 + 1;
+    // s-major: entry (s-1)*ell + j = w_K^{j s}
+    const long long ell = 1LL << (logK - logR);
+    long long s = idx / ell + 1, j = idx % ell;
     long long E = (j * s) & ((1LL << logK) - 1);
     double x = -2.0 * (double)E / (double)(1LL << logK);
     double sn, cs;
@@ -358,8 +481,75 @@ static int launch_special(const PassDesc& d, int elem_bytes, int b2, long long g
   return set_error(PAC_ERROR_INTERNAL, "no specialised kernel for a pass marked special");
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no -lcuda)
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+  });
+  return fn;
+}
+
+// 3D view (S columns, L rows, O outer) of a column pass's array; box W x BOXR
+static int col_tensor_map(CUtensorMap* m, const void* base, int esz, const PassDesc& d) {
+  auto enc = tensor_map_encoder();
+  if (!enc) return set_error(PAC_ERROR_CUDA, "cuTensorMapEncodeTiled unavailable");
+  const cuuint64_t S = 1ull << d.logS, L = 1ull << d.logL;
+  cuuint64_t dims[3] = {S, L, (cuuint64_t)(d.nlines >> d.logS)};
+  cuuint64_t strides[2] = {S * esz, S * L * esz};
+  cuuint32_t box[3] = {(cuuint32_t)d.W, (cuuint32_t)tma_boxr(d.logL), 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = enc(m, esz == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                   3, const_cast<void*>(base), dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return set_error(PAC_ERROR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return PAC_SUCCESS;
+}
+
+static int launch_tma(const PassDesc& d, int elem_bytes, int b2, long long grid, int threads,
+                      size_t smem, void* stream) {
+  CUtensorMap m[4];
+  PAC_TRY_BE(col_tensor_map(&m[0], d.in_re, elem_bytes, d));
+  PAC_TRY_BE(col_tensor_map(&m[1], d.in_im, elem_bytes, d));
+  PAC_TRY_BE(col_tensor_map(&m[2], d.out_re, elem_bytes, d));
+  PAC_TRY_BE(col_tensor_map(&m[3], d.out_im, elem_bytes, d));
+#define PAC_X(T, BY, B2_, MO, SG, LL, LW, NT_, MB)                                             \
+  if (elem_bytes == BY && b2 == B2_ && d.mode == MO && d.sign == SG && d.logL == LL &&      \
+      d.W == (1 << LW) && threads == NT_) {                                                 \
+    static std::mutex mu;                                                                   \
+    static std::set<int> configured;                                                        \
+    auto kern = pac_tma_col_kernel<T, B2_, MO, SG, LL, LW, NT_, MB>;                        \
+    if (smem > 48 * 1024) {                                                                 \
+      int dev = 0;                                                                          \
+      cudaGetDevice(&dev);                                                                  \
+      std::lock_guard<std::mutex> g(mu);                                                    \
+      if (!configured.count(dev)) {                                                         \
+        PAC_CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,      \
+                                    (int)smem),                                             \
+               "cudaFuncSetAttribute");                                                     \
+        configured.insert(dev);                                                             \
+      }                                                                                     \
+    }                                                                                       \
+    kern<<<(unsigned)grid, threads, smem, (cudaStream_t)stream>>>(d, m[0], m[1], m[2], m[3]); \
+    PAC_CU(cudaGetLastError(), "pac_tma_col_kernel launch");                                \
+    g_launches.fetch_add(1, std::memory_order_relaxed);                                     \
+    return PAC_SUCCESS;                                                                     \
+  }
+  PAC_TMA_LIST(PAC_X)
+#undef PAC_X
+  return set_error(PAC_ERROR_INTERNAL, "no TMA kernel for a pass marked tma");
+}
+
 int be_launch_pass(const PassDesc& d, int elem_bytes, int b2, long long grid, int threads,
                    size_t smem, void* stream) {
+  if (d.tma) return launch_tma(d, elem_bytes, b2, grid, threads, smem, stream);
   if (d.spec) {
     bool done = false;
     return launch_special(d, elem_bytes, b2, grid, threads, smem, stream, &done);

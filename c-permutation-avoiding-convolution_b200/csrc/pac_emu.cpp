@@ -91,8 +91,55 @@ static void replay_special(const PassDesc& d, long long grid) {
   }
 }
 
+// replay of a TMA column kernel: the tile is copied into the swizzled dense
+// layout the tensor copy writes, transformed in place, and copied back
+template <typename T, int B2, int MODE, int SIGN, int LOGL, int LOGW, int NT>
+static void replay_tma(const PassDesc& d, long long grid) {
+  constexpr int W = 1 << LOGW, L = 1 << LOGL;
+  using SP = TmaShape<LOGL, LOGW, (int)sizeof(T)>;
+  std::vector<T> sm((size_t)2 * W * L);
+  T* sre = sm.data();
+  T* sim = sre + (size_t)W * L;
+  std::vector<long long> lb(W);
+  const T* ire = (const T*)d.in_re;
+  const T* iim = (const T*)d.in_im;
+  T* ore = (T*)d.out_re;
+  T* oim = (T*)d.out_im;
+  for (long long cta = 0; cta < grid; ++cta) {
+    for (int w = 0; w < W; ++w) lb[w] = line_base(d, cta * W + w);
+    for (int w = 0; w < W; ++w)
+      for (int e = 0; e < L; ++e) {
+        long long gi = lb[w] + ((long long)e << d.logS);
+        int si = SP::template sm<T>(d, w, e);
+        sre[si] = ire[gi];
+        sim[si] = iim[gi];
+      }
+    pass_body_ct<T, B2, MODE, SIGN, SP, NT, RadsFor<LOGL, B2>, true>(d, cta, sre, sim, lb.data(),
+                                                                     lb.data());
+    for (int w = 0; w < W; ++w)
+      for (int e = 0; e < L; ++e) {
+        long long gi = lb[w] + ((long long)e << d.logS);
+        int si = SP::template sm<T>(d, w, e);
+        ore[gi] = sre[si];
+        oim[gi] = sim[si];
+      }
+  }
+}
+
 int be_launch_pass(const PassDesc& d, int elem_bytes, int b2, long long grid, int threads,
                    size_t, void*) {
+  if (d.tma) {
+#define PAC_X(T, BY, B2_, MO, SG, LL, LW, NT_, MB)                                         \
+  if (elem_bytes == BY && b2 == B2_ && d.mode == MO && d.sign == SG && d.logL == LL &&  \
+      d.W == (1 << LW) && threads == NT_) {                                             \
+    replay_tma<T, B2_, MO, SG, LL, LW, NT_>(d, grid);                                   \
+    g_launches++;                                                                       \
+    return PAC_SUCCESS;                                                                 \
+  }
+    PAC_TMA_LIST(PAC_X)
+#undef PAC_X
+    return set_error(PAC_ERROR_INTERNAL, "no TMA replay for a pass marked tma");
+  }
   if (d.spec) {
     const int cols = d.logS > 0 ? 1 : 0;
 #define PAC_X(T, BY, B2_, MO, SG, LL, CO, LW, NT_, MB)                                        \
@@ -138,7 +185,9 @@ int be_fill_stage_tw(void* dst, int elem_bytes, int logK, int logR, void*) {
   long long R1 = (1LL << logR) - 1, K = 1LL << logK;
   long long n = (K >> logR) * R1;
   for (long long idx = 0; idx < n; ++idx) {
-    long long j = idx / R1, s = idx % R1 + 1;
+    long long ell = K >> logR;  // s-major: entry (s-1)*ell + j = w_K^{j s}
+    long long s = idx / ell + 1, j = idx % ell;
+    (void)R1;
     double c, sn;
     root((j * s) % K, K, &c, &sn);
     if (elem_bytes == 8) put<double>(dst, idx, c, sn);

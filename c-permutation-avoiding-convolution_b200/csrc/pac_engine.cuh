@@ -85,6 +85,8 @@ struct PassDesc {
   int* status;
   // 1: this pass runs the kernel specialised for its geometry (pac_special.h)
   int spec;
+  // 1: the specialised column kernel moves its tile with TMA (pac_special.h)
+  int tma;
 };
 
 // ---------------------------------------------------------------------------

@@ -62,6 +62,31 @@ PAC_HDC int pitch_for(int bytes, int logL, int W) {
   X(float, 4, 1, MODE_DIF, -1, 11, 1, 2, 512, 1)           \
   X(float, 4, 1, MODE_DIT, +1, 11, 1, 2, 512, 1)
 
+// Column passes whose tile is moved by TMA (tensor copies into a 128-byte
+// swizzled dense tile, PassDesc.tma): rows of W * 8 or W * 4 = 16 bytes.
+// fields: element type, bytes, log2 digit base, mode, sign, log2 L, log2 W,
+// threads, min CTAs per SM
+#define PAC_TMA_LIST(X)                                    \
+  X(double, 8, 1, MODE_DIF, -1, 11, 1, 256, 2)             \
+  X(double, 8, 1, MODE_DIT, +1, 11, 1, 256, 2)             \
+  X(float, 4, 1, MODE_DIF, -1, 11, 2, 512, 1)              \
+  X(float, 4, 1, MODE_DIT, +1, 11, 2, 512, 1)
+
+// rows of the TMA box (the tensor map's box height; a tile is L / TMA_BOXR boxes)
+PAC_HDC int tma_boxr(int logL) { return logL > 8 ? 256 : (1 << logL); }
+
+inline bool tma_geometry(int bytes, int b2, int mode, int sign, int logL, int* logW, int* nt) {
+#define PAC_X(T, BY, B2_, MO, SG, LL, LW, NT_, MB)                                  \
+  if (bytes == BY && b2 == B2_ && mode == MO && sign == SG && logL == LL) {      \
+    *logW = LW;                                                                  \
+    *nt = NT_;                                                                   \
+    return true;                                                                 \
+  }
+  PAC_TMA_LIST(PAC_X)
+#undef PAC_X
+  return false;
+}
+
 inline bool special_geometry(int bytes, int b2, int mode, int sign, int logL, int cols,
                              int* logW, int* nt) {
 #define PAC_X(T, BY, B2_, MO, SG, LL, CO, LW, NT_, MB)                                    \

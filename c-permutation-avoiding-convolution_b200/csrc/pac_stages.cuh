@@ -44,8 +44,42 @@ struct Shape {
     if constexpr (COLS_ >= 0) return COLS_ != 0;
     else return d.logS > 0;
   }
+  // threads take consecutive lines first: only where a stage touches global
+  // memory of a column tile (coalesced rows of W elements)
+  static PAC_HD bool wfast(const PassDesc& d, bool global_facing) {
+    return global_facing && cols(d);
+  }
+  // shared-memory index of element e of line w: padded lines
+  template <typename T>
+  static PAC_HD int sm(const PassDesc& d, int w, int e) {
+    return w * pitch(d) + sidx<T>(e);
+  }
 };
 using RtShape = Shape<>;
+
+// Column tile moved by TMA: dense [L][W] tile in the 128-byte swizzled order
+// the tensor copy writes (16-byte chunk index, address bits 4-6, XOR-ed with
+// bits 7-9).  Threads take consecutive lines first in every stage, which
+// makes all stage accesses bank-conflict-free for W * ESZ = 16 bytes.
+template <int LOGL_, int LOGW_, int ESZ>
+struct TmaShape {
+  static constexpr int kLogL = LOGL_;
+  static constexpr int kLogW = LOGW_;
+  static constexpr int kPitch = 0;
+  static constexpr int kCols = 1;
+  static PAC_HD int logL(const PassDesc&) { return LOGL_; }
+  static PAC_HD int logW(const PassDesc&) { return LOGW_; }
+  static PAC_HD int W(const PassDesc&) { return 1 << LOGW_; }
+  static PAC_HD int pitch(const PassDesc&) { return 0; }
+  static PAC_HD bool cols(const PassDesc&) { return true; }
+  static PAC_HD bool wfast(const PassDesc&, bool) { return true; }
+  template <typename T>
+  static PAC_HD int sm(const PassDesc&, int w, int e) {
+    uint32_t b = (uint32_t)((e << LOGW_) + w) * ESZ;
+    b ^= ((b >> 7) & 7u) << 4;
+    return (int)(b / ESZ);
+  }
+};
 
 // butterfly index -> (w, blk, j) for a stage of block 2^logK, radix 2^logR
 template <class SP>
@@ -54,7 +88,7 @@ PAC_HD void bf_coords(const PassDesc& d, int logK, int logR, bool global_facing,
   const int lbf = SP::logL(d) - logR;  // butterflies per line (log)
   const int logell = logK - logR;
   int v;
-  if (global_facing && SP::cols(d)) {
+  if (SP::wfast(d, global_facing)) {
     // consecutive threads take consecutive columns: coalesced rows of W
     *w = u & (SP::W(d) - 1);
     v = u >> SP::logW(d);
@@ -91,7 +125,6 @@ PAC_HD void stage_bf(const PassDesc& d, long long cta, T* sre, T* sim, int logK_
   bf_coords<SP>(d, logK, LR, src == IO_GLOBAL || dst == IO_GLOBAL, u, &w, &blk, &j);
   const int ell = 1 << logell;
   const int e0 = (blk << logK) + j;
-  const int pitch = SP::pitch(d);
   const T* ire = (const T*)d.in_re;
   const T* iim = (const T*)d.in_im;
   Cx<T> x[R];
@@ -104,11 +137,13 @@ PAC_HD void stage_bf(const PassDesc& d, long long cta, T* sre, T* sim, int logK_
       long long gi = lbase_in[w] + ((long long)e << d.logS);
       x[m] = Cx<T>{ld_g(ire + gi), ld_g(iim + gi)};
     } else {
-      int si = w * pitch + sidx<T>(e);
+      int si = SP::template sm<T>(d, w, e);
       x[m] = Cx<T>{sre[si], sim[si]};
     }
   });
-  const Cx<T>* tw = (const Cx<T>*)d.tw + twoff + j * (R - 1);
+  // stage table, s-major: entry (s-1)*ell + j = w_K^{j s}; for one s the
+  // threads of a warp read consecutive j (coalesced)
+  const Cx<T>* tw = (const Cx<T>*)d.tw + twoff + j;
   const bool twiddle = logell > 0 && j > 0;
   if constexpr (!DIF) {
     // 4-step pre-twiddle: only the innermost stage (ell == 1) of a DIT pass
@@ -121,7 +156,7 @@ PAC_HD void stage_bf(const PassDesc& d, long long cta, T* sre, T* sim, int logK_
     if (twiddle) {
       static_for<R - 1>([&](auto ss) {
         constexpr int s = ss.value + 1;
-        x[s] = ctw(x[s], ld_tw(tw + (s - 1)), SIGN);
+        x[s] = ctw(x[s], ld_tw(tw + (s - 1) * ell), SIGN);
       });
     }
   }
@@ -131,7 +166,7 @@ PAC_HD void stage_bf(const PassDesc& d, long long cta, T* sre, T* sim, int logK_
     if (twiddle) {
       static_for<R>([&](auto pp) {
         constexpr int s = brev_c(pp.value, LR);
-        if constexpr (s > 0) x[pp.value] = ctw(x[pp.value], ld_tw(tw + (s - 1)), SIGN);
+        if constexpr (s > 0) x[pp.value] = ctw(x[pp.value], ld_tw(tw + (s - 1) * ell), SIGN);
       });
     }
     // 4-step post-twiddle: only the innermost stage of a DIF pass
@@ -159,7 +194,7 @@ PAC_HD void stage_bf(const PassDesc& d, long long cta, T* sre, T* sim, int logK_
       ore[gi] = v.re;
       oim[gi] = v.im;
     } else {
-      int si = w * pitch + sidx<T>(e);
+      int si = SP::template sm<T>(d, w, e);
       sre[si] = v.re;
       sim[si] = v.im;
     }
@@ -176,7 +211,6 @@ PAC_HD void middle_bf(const PassDesc& d, T* sre, T* sim, int src, int dst, int u
   int w, blk, j;
   bf_coords<SP>(d, LR, LR, src == IO_GLOBAL || dst == IO_GLOBAL, u, &w, &blk, &j);
   const int e0 = blk << LR;  // ell == 1, j == 0
-  const int pitch = SP::pitch(d);
   const T* ire = (const T*)d.in_re;
   const T* iim = (const T*)d.in_im;
   const T* hre = (const T*)d.h_re;
@@ -189,7 +223,7 @@ PAC_HD void middle_bf(const PassDesc& d, T* sre, T* sim, int src, int dst, int u
       long long gi = lbase[w] + ((long long)e << d.logS);
       x[m] = Cx<T>{ld_g(ire + gi), ld_g(iim + gi)};
     } else {
-      int si = w * pitch + sidx<T>(e);
+      int si = SP::template sm<T>(d, w, e);
       x[m] = Cx<T>{sre[si], sim[si]};
     }
   });
@@ -217,7 +251,7 @@ PAC_HD void middle_bf(const PassDesc& d, T* sre, T* sim, int src, int dst, int u
       ore[gi] = y[p].re;
       oim[gi] = y[p].im;
     } else {
-      int si = w * pitch + sidx<T>(e);
+      int si = SP::template sm<T>(d, w, e);
       sre[si] = y[p].re;
       sim[si] = y[p].im;
     }
@@ -410,9 +444,12 @@ struct Rads {
 #define PAC_FOR_BF_CT(n, NT, u) for (int u = 0; u < (n); ++u)
 #endif
 
-template <typename T, int B2, int MODE, int SIGN, class SP, int NT, class RS>
+// SMEM_IO: the tile is already in shared memory (TMA) and is written back
+// there; the first and last stages then read/write shared memory.
+template <typename T, int B2, int MODE, int SIGN, class SP, int NT, class RS, bool SMEM_IO = false>
 PAC_HD void pass_body_ct(const PassDesc& d, long long cta, T* sre, T* sim, const long long* lbi,
                          const long long* lbo) {
+  constexpr int GIO = SMEM_IO ? IO_SMEM : IO_GLOBAL;
   constexpr int LOGL = SP::kLogL;
   constexpr int LOGW = SP::kLogW;
   static_assert(LOGL >= 0 && LOGW >= 0 && SP::kPitch >= 0 && SP::kCols >= 0, "fixed shape");
@@ -426,8 +463,8 @@ PAC_HD void pass_body_ct(const PassDesc& d, long long cta, T* sre, T* sim, const
       if constexpr (i > 0) PAC_SYNC();
       PAC_FOR_BF_CT(nbf, NT, u) {
         stage_bf<T, B2, (1 << LRr), SIGN, true, SP, LK>(
-            d, cta, sre, sim, LK, d.tw_off[i], i == 0 ? IO_GLOBAL : IO_SMEM,
-            i == n - 1 ? IO_GLOBAL : IO_SMEM, u, lbi, lbo);
+            d, cta, sre, sim, LK, d.tw_off[i], i == 0 ? GIO : IO_SMEM,
+            i == n - 1 ? GIO : IO_SMEM, u, lbi, lbo);
       }
     });
   } else if constexpr (MODE == MODE_DIT) {
@@ -440,8 +477,8 @@ PAC_HD void pass_body_ct(const PassDesc& d, long long cta, T* sre, T* sim, const
       if constexpr (k > 0) PAC_SYNC();
       PAC_FOR_BF_CT(nbf, NT, u) {
         stage_bf<T, B2, (1 << LRr), SIGN, false, SP, LK>(
-            d, cta, sre, sim, LK, d.tw_off[i], k == 0 ? IO_GLOBAL : IO_SMEM,
-            k == n - 1 ? IO_GLOBAL : IO_SMEM, u, lbi, lbo);
+            d, cta, sre, sim, LK, d.tw_off[i], k == 0 ? GIO : IO_SMEM,
+            k == n - 1 ? GIO : IO_SMEM, u, lbi, lbo);
       }
     });
   } else {
@@ -453,13 +490,13 @@ PAC_HD void pass_body_ct(const PassDesc& d, long long cta, T* sre, T* sim, const
       if constexpr (i > 0) PAC_SYNC();
       PAC_FOR_BF_CT(nbf, NT, u) {
         stage_bf<T, B2, (1 << LRr), -1, true, SP, LK>(
-            d, cta, sre, sim, LK, d.tw_off[i], i == 0 ? IO_GLOBAL : IO_SMEM, IO_SMEM, u, lbi, lbo);
+            d, cta, sre, sim, LK, d.tw_off[i], i == 0 ? GIO : IO_SMEM, IO_SMEM, u, lbi, lbo);
       }
     });
     {
       constexpr int LRr = RS::v[n - 1];
       constexpr int nbf = 1 << (LOGW + LOGL - LRr);
-      constexpr int io = n == 1 ? IO_GLOBAL : IO_SMEM;
+      constexpr int io = n == 1 ? GIO : IO_SMEM;
       if constexpr (n > 1) PAC_SYNC();
       PAC_FOR_BF_CT(nbf, NT, u) { middle_bf<T, B2, (1 << LRr), SP>(d, sre, sim, io, io, u, lbi); }
     }
@@ -471,7 +508,7 @@ PAC_HD void pass_body_ct(const PassDesc& d, long long cta, T* sre, T* sim, const
       PAC_SYNC();
       PAC_FOR_BF_CT(nbf, NT, u) {
         stage_bf<T, B2, (1 << LRr), +1, false, SP, LK>(
-            d, cta, sre, sim, LK, d.tw_off[i], IO_SMEM, i == 0 ? IO_GLOBAL : IO_SMEM, u, lbi, lbo);
+            d, cta, sre, sim, LK, d.tw_off[i], IO_SMEM, i == 0 ? GIO : IO_SMEM, u, lbi, lbo);
       }
     });
   }
