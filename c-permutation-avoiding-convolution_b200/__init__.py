@@ -78,6 +78,7 @@ def _declare(L):
     L.pac_stream_create.argtypes = [C.POINTER(_vp)]
     L.pac_stream_destroy.argtypes = [_vp]
     L.pac_stream_wait_stream.argtypes = [_vp, _vp]
+    L.pac_stream_set_l2_persisting.argtypes = [_vp, _vp, sz]
     L.pac_launch_count.restype = ll
     L.pac_status_string.restype = C.c_char_p
     L.pac_status_string.argtypes = [i]

@@ -23,6 +23,7 @@ int be_stream_create(void** s);
 int be_stream_destroy(void* s);
 int be_stream_sync(void* s);
 int be_stream_wait(void* waiter, void* waitee);
+int be_l2_persist(void* stream, const void* base, size_t bytes);
 // timing events: record on a stream, elapsed milliseconds between two
 int be_event_create(void** ev);
 int be_event_destroy(void* ev);

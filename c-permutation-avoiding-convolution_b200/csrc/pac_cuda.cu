@@ -12,6 +12,7 @@
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 #include <stdio.h>
+#include <string.h>
 
 #include <atomic>
 #include <mutex>
@@ -376,6 +377,31 @@ int be_stream_sync(void* s) {
   PAC_CU(cudaStreamSynchronize((cudaStream_t)s), "cudaStreamSynchronize");
   return PAC_SUCCESS;
 }
+int be_l2_persist(void* stream, const void* base, size_t bytes) {
+  int dev = 0;
+  PAC_CU(cudaGetDevice(&dev), "cudaGetDevice");
+  cudaDeviceProp prop;
+  PAC_CU(cudaGetDeviceProperties(&prop, dev), "cudaGetDeviceProperties");
+  cudaStreamAttrValue v;
+  memset(&v, 0, sizeof(v));
+  if (bytes > 0 && prop.persistingL2CacheMaxSize > 0) {
+    size_t limit = bytes < (size_t)prop.persistingL2CacheMaxSize ? bytes
+                                                                  : (size_t)prop.persistingL2CacheMaxSize;
+    PAC_CU(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, limit), "cudaDeviceSetLimit");
+    size_t win = bytes < (size_t)prop.accessPolicyMaxWindowSize ? bytes
+                                                                : (size_t)prop.accessPolicyMaxWindowSize;
+    v.accessPolicyWindow.base_ptr = const_cast<void*>(base);
+    v.accessPolicyWindow.num_bytes = win;
+    v.accessPolicyWindow.hitRatio = (float)((double)limit / (double)win > 1.0 ? 1.0 : (double)limit / (double)win);
+    v.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+    v.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+  }
+  PAC_CU(cudaStreamSetAttribute((cudaStream_t)stream, cudaStreamAttributeAccessPolicyWindow, &v),
+         "cudaStreamSetAttribute");
+  if (bytes == 0) cudaCtxResetPersistingL2Cache();
+  return PAC_SUCCESS;
+}
+
 int be_event_create(void** ev) {
   cudaEvent_t e;
   PAC_CU(cudaEventCreate(&e), "cudaEventCreate");

@@ -49,6 +49,7 @@ int be_stream_create(void** s) {
 int be_stream_destroy(void*) { return PAC_SUCCESS; }
 int be_stream_sync(void*) { return PAC_SUCCESS; }
 int be_stream_wait(void*, void*) { return PAC_SUCCESS; }
+int be_l2_persist(void*, const void*, size_t) { return PAC_SUCCESS; }
 int be_event_create(void** ev) {
   *ev = nullptr;
   return PAC_SUCCESS;

@@ -804,6 +804,12 @@ PAC_API int pac_stream_create(pac_stream_t* s) {
 }
 PAC_API int pac_stream_destroy(pac_stream_t s) { return be_stream_destroy(s); }
 PAC_API int pac_stream_synchronize(pac_stream_t s) { return be_stream_sync(s); }
+PAC_API int pac_stream_set_l2_persisting(pac_stream_t stream, const void* base, size_t bytes) {
+  if (bytes > 0 && !base)
+    return set_error(PAC_ERROR_INVALID_VALUE, "pac_stream_set_l2_persisting: NULL base");
+  PAC_TRY(be_init());
+  return be_l2_persist(stream, base, bytes);
+}
 PAC_API int pac_stream_wait_stream(pac_stream_t waiter, pac_stream_t waitee) {
   return be_stream_wait(waiter, waitee);
 }

@@ -62,15 +62,14 @@ PAC_HDC int pitch_for(int bytes, int logL, int W) {
   X(float, 4, 1, MODE_DIF, -1, 11, 1, 2, 512, 1)           \
   X(float, 4, 1, MODE_DIT, +1, 11, 1, 2, 512, 1)
 
-// Column passes whose tile is moved by TMA (tensor copies into a 128-byte
-// swizzled dense tile, PassDesc.tma): rows of W * 8 or W * 4 = 16 bytes.
+// Column passes whose tile is moved by TMA (PassDesc.tma).  Empty: with the
+// 128-byte swizzle the tensor copy pads every box row to 128 bytes in shared
+// memory, so a 16-byte-wide column tile would need 8x its size; a dense
+// (unswizzled) tile makes the innermost stage's accesses 8-way bank
+// conflicted.  No column geometry is served by TMA until a layout is both.
 // fields: element type, bytes, log2 digit base, mode, sign, log2 L, log2 W,
 // threads, min CTAs per SM
-#define PAC_TMA_LIST(X)                                    \
-  X(double, 8, 1, MODE_DIF, -1, 11, 1, 256, 2)             \
-  X(double, 8, 1, MODE_DIT, +1, 11, 1, 256, 2)             \
-  X(float, 4, 1, MODE_DIF, -1, 11, 2, 512, 1)              \
-  X(float, 4, 1, MODE_DIT, +1, 11, 2, 512, 1)
+#define PAC_TMA_LIST(X)
 
 // rows of the TMA box (the tensor map's box height; a tile is L / TMA_BOXR boxes)
 PAC_HDC int tma_boxr(int logL) { return logL > 8 ? 256 : (1 << logL); }

@@ -181,6 +181,13 @@ PAC_API int pac_stream_synchronize(pac_stream_t stream);
  * on `waitee` has finished (an event recorded on waitee). */
 PAC_API int pac_stream_wait_stream(pac_stream_t waiter, pac_stream_t waitee);
 
+/* Keep [base, base + bytes) resident in L2 for work queued on `stream`
+ * (CUDA access-policy window, persisting hits, streaming misses; the
+ * persisting set-aside is a limit of this process's context only).
+ * Meant for the convolution output, which the passes of pac_convolve use as
+ * their intermediate.  bytes == 0 removes the window. */
+PAC_API int pac_stream_set_l2_persisting(pac_stream_t stream, const void* base, size_t bytes);
+
 /* Per-pass timing: while enabled, pac_convolve and pac_transform record a
  * CUDA event before the first and after every pass on the caller's stream
  * and wait for them at the end of the call (so calls become synchronous).
