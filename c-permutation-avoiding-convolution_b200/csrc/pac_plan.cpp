@@ -312,7 +312,11 @@ static void apply_special(const Schedule& s, PassSpec& p) {
     p.smem = (size_t)2 * d.W * d.L * s.bytes + 1024;
     return;
   }
-  if (!special_geometry(s.bytes, s.b2, d.mode, d.sign, d.logL, d.logS > 0 ? 1 : 0, &logW, &nt))
+  const char* var = getenv("PAC_SPECIAL_VARIANT");
+  const int variant = var ? atoi(var) : 0;
+  if (!special_geometry(s.bytes, s.b2, d.mode, d.sign, d.logL, d.logS > 0 ? 1 : 0, &logW, &nt,
+                        variant) &&
+      !special_geometry(s.bytes, s.b2, d.mode, d.sign, d.logL, d.logS > 0 ? 1 : 0, &logW, &nt))
     return;
   const long long W = 1LL << logW;
   if ((d.nlines & (W - 1)) != 0) return;

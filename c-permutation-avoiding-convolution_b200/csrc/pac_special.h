@@ -60,7 +60,13 @@ PAC_HDC int pitch_for(int bytes, int logL, int W) {
   X(double, 8, 1, MODE_DIT, +1, 11, 1, 1, 256, 2)          \
   X(float, 4, 1, MODE_CONV, 0, 11, 0, 1, 256, 2)           \
   X(float, 4, 1, MODE_DIF, -1, 11, 1, 2, 512, 1)           \
-  X(float, 4, 1, MODE_DIT, +1, 11, 1, 2, 512, 1)
+  X(float, 4, 1, MODE_DIT, +1, 11, 1, 2, 512, 1)           \
+  X(float, 4, 1, MODE_DIF, -1, 11, 1, 2, 256, 2)           \
+  X(float, 4, 1, MODE_DIT, +1, 11, 1, 2, 256, 2)           \
+  X(float, 4, 1, MODE_DIF, -1, 11, 1, 3, 512, 1)           \
+  X(float, 4, 1, MODE_DIT, +1, 11, 1, 3, 512, 1)
+// (a geometry may have several candidates; the first is the default and
+// PAC_SPECIAL_VARIANT=k selects the k-th, for tuning)
 
 // Column passes whose tile is moved by TMA (PassDesc.tma).  Empty: with the
 // 128-byte swizzle the tensor copy pads every box row to 128 bytes in shared
@@ -87,10 +93,11 @@ inline bool tma_geometry(int bytes, int b2, int mode, int sign, int logL, int* l
 }
 
 inline bool special_geometry(int bytes, int b2, int mode, int sign, int logL, int cols,
-                             int* logW, int* nt) {
+                             int* logW, int* nt, int variant = 0) {
+  int seen = 0;
 #define PAC_X(T, BY, B2_, MO, SG, LL, CO, LW, NT_, MB)                                    \
   if (bytes == BY && b2 == B2_ && mode == MO && (MO == MODE_CONV || sign == SG) &&     \
-      logL == LL && cols == CO) {                                                      \
+      logL == LL && cols == CO && seen++ == variant) {                                 \
     *logW = LW;                                                                        \
     *nt = NT_;                                                                         \
     return true;                                                                       \
