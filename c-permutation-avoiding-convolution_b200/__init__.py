@@ -63,6 +63,7 @@ def _declare(L):
     L.pac_plan_destroy.argtypes = [_vp]
     L.pac_filter_spectrum.argtypes = [_vp, _vp, _vp, i, _vp, _vp, d, _vp]
     L.pac_convolve.argtypes = [_vp, _vp, _vp, _vp, _vp, i, _vp, _vp, d, _vp]
+    L.pac_spectrum_to_plan_order.argtypes = [_vp, _vp, _vp, i, _vp, _vp, d, _vp]
     L.pac_transform.argtypes = [_vp, i, _vp, _vp, _vp, _vp, _vp]
     if hasattr(L, "pac_convolve_1d_noalloc"):  # product library only
         L.pac_convolve_1d_noalloc.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, i, i, _vp]

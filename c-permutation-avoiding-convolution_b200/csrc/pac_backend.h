@@ -41,6 +41,12 @@ int be_fill_pow_tw(void* dst, int elem_bytes, long long count, long long stride,
 // reference-layout tables of t levels for radix r (r^t - 1 entries)
 int be_fill_ref_tw(int r, int t, double* re, double* im, void* stream);
 int be_round_to_f32(const double* src, float* dst, long long n, void* stream);
+// P-order FP64 spectrum lines (length 2^logL) -> plan order (every block of
+// 2^logR positions transposed to stride L/R), scaled, stored as elem_bytes;
+// in == out allowed for elem_bytes 8
+int be_plan_order(const double* in_re, const double* in_im, void* out_re, void* out_im,
+                  int elem_bytes, int logL, int logR, long long nlines, double scale,
+                  void* stream);
 // y = scale * x .* h[i & hmask] (complex, split); elem_bytes 8 or 4
 int be_pointwise(long long n, int elem_bytes, const void* xr, const void* xi, const void* hr,
                  const void* hi, long long hmask, void* yr, void* yi, double scale,

@@ -249,6 +249,31 @@ __global__ void fill_ref_tw_kernel(int r, int t, double* re, double* im) {
   }
 }
 
+// P order -> plan order, one line per CTA iteration through shared memory
+// (the whole line is read before any of it is written, so in == out works)
+template <typename Tout>
+__global__ void plan_order_kernel(const double* in_re, const double* in_im, Tout* out_re,
+                                  Tout* out_im, int logL, int logR, long long nlines,
+                                  double scale) {
+  extern __shared__ double pbuf[];
+  const int L = 1 << logL, lq = logL - logR;
+  for (long long line = blockIdx.x; line < nlines; line += gridDim.x) {
+    const long long base = line << logL;
+    for (int q = threadIdx.x; q < L; q += blockDim.x) {
+      pbuf[q] = in_re[base + q];
+      pbuf[L + q] = in_im[base + q];
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < L; idx += blockDim.x) {
+      const int t = idx >> lq, blk = idx & ((1 << lq) - 1);
+      const int q = (blk << logR) + t;
+      out_re[base + idx] = (Tout)(pbuf[q] * scale);
+      out_im[base + idx] = (Tout)(pbuf[L + q] * scale);
+    }
+    __syncthreads();
+  }
+}
+
 __global__ void round_f32_kernel(const double* src, float* dst, long long n) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
@@ -625,6 +650,45 @@ int be_fill_ref_tw(int r, int t, double* re, double* im, void* stream) {
   for (int q = 0; q < t; ++q) total *= r;
   fill_ref_tw_kernel<<<grid_for(total), 256, 0, (cudaStream_t)stream>>>(r, t, re, im);
   PAC_LAUNCHED("fill_ref_tw");
+  return PAC_SUCCESS;
+}
+
+int be_plan_order(const double* in_re, const double* in_im, void* out_re, void* out_im,
+                  int elem_bytes, int logL, int logR, long long nlines, double scale,
+                  void* stream) {
+  static std::mutex mu;
+  static std::set<std::pair<int, int>> configured;
+  const size_t smem = (size_t)2 * sizeof(double) << logL;
+  long long grid = nlines < 148 * 8 ? nlines : 148 * 8;
+  if (grid < 1) grid = 1;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (elem_bytes == 8) {
+    if (smem > 48 * 1024) {
+      std::lock_guard<std::mutex> g(mu);
+      if (!configured.count({dev, 8})) {
+        PAC_CU(cudaFuncSetAttribute(plan_order_kernel<double>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024),
+               "cudaFuncSetAttribute");
+        configured.insert({dev, 8});
+      }
+    }
+    plan_order_kernel<double><<<(unsigned)grid, 256, smem, (cudaStream_t)stream>>>(
+        in_re, in_im, (double*)out_re, (double*)out_im, logL, logR, nlines, scale);
+  } else {
+    if (smem > 48 * 1024) {
+      std::lock_guard<std::mutex> g(mu);
+      if (!configured.count({dev, 4})) {
+        PAC_CU(cudaFuncSetAttribute(plan_order_kernel<float>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024),
+               "cudaFuncSetAttribute");
+        configured.insert({dev, 4});
+      }
+    }
+    plan_order_kernel<float><<<(unsigned)grid, 256, smem, (cudaStream_t)stream>>>(
+        in_re, in_im, (float*)out_re, (float*)out_im, logL, logR, nlines, scale);
+  }
+  PAC_LAUNCHED("plan_order");
   return PAC_SUCCESS;
 }
 

@@ -264,12 +264,15 @@ static void run_pac_conv(const char* fn, int rank, const int* dims, int r, doubl
    * signal's H2D run in opposite directions and overlap. */
   TRY(pac_memcpy_h2d(hr, h_re, nb, e->s1));
   TRY(pac_memcpy_h2d(hi, h_im, nb, e->s1));
-  TRY(pac_filter_spectrum(e->plan, hr, hi, 1, hr, hi, 1.0, e->s1));
+  /* A^T h in the reference's order goes back to the caller; the same
+   * buffer is then reordered in place into the plan's spectrum order */
+  TRY(pac_transform(e->plan, PAC_OP_AT, hr, hi, hr, hi, e->s1));
   TRY(pac_memcpy_h2d(xr, re, nb, e->s2));
   TRY(pac_memcpy_h2d(xi, im, nb, e->s2));
-  TRY(pac_stream_wait_stream(e->s2, e->s1));
   TRY(pac_memcpy_d2h(h_re, hr, nb, e->s1));
   TRY(pac_memcpy_d2h(h_im, hi, nb, e->s1));
+  TRY(pac_spectrum_to_plan_order(e->plan, hr, hi, 1, hr, hi, 1.0, e->s1));
+  TRY(pac_stream_wait_stream(e->s2, e->s1));
   TRY(pac_convolve(e->plan, xr, xi, hr, hi, 0, xr, xi, 1.0 / (double)N, e->s2));
   TRY(pac_memcpy_d2h(re, xr, nb, e->s2));
   TRY(pac_memcpy_d2h(im, xi, nb, e->s2));

@@ -225,6 +225,32 @@ int be_fill_ref_tw(int r, int t, double* re, double* im, void*) {
   return PAC_SUCCESS;
 }
 
+int be_plan_order(const double* in_re, const double* in_im, void* out_re, void* out_im,
+                  int elem_bytes, int logL, int logR, long long nlines, double scale, void*) {
+  const int L = 1 << logL, lq = logL - logR;
+  std::vector<double> br(L), bi(L);
+  for (long long line = 0; line < nlines; ++line) {
+    const long long base = line << logL;
+    for (int q = 0; q < L; ++q) {
+      br[q] = in_re[base + q];
+      bi[q] = in_im[base + q];
+    }
+    for (int idx = 0; idx < L; ++idx) {
+      const int t = idx >> lq, blk = idx & ((1 << lq) - 1);
+      const int q = (blk << logR) + t;
+      if (elem_bytes == 8) {
+        ((double*)out_re)[base + idx] = br[q] * scale;
+        ((double*)out_im)[base + idx] = bi[q] * scale;
+      } else {
+        ((float*)out_re)[base + idx] = (float)(br[q] * scale);
+        ((float*)out_im)[base + idx] = (float)(bi[q] * scale);
+      }
+    }
+  }
+  g_launches++;
+  return PAC_SUCCESS;
+}
+
 int be_round_to_f32(const double* src, float* dst, long long n, void*) {
   for (long long i = 0; i < n; ++i) dst[i] = (float)src[i];
   g_launches++;

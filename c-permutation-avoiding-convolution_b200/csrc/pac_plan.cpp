@@ -513,6 +513,27 @@ static int run_conv(pac_plan_s* pl, const void* x_re, const void* x_im, const vo
   return exec_passes(pl, s, passes, stream);
 }
 
+// P-order FP64 spectrum -> the plan's spectrum storage: every block of R
+// positions (R the last stage radix of the innermost factor, the one the
+// fused pass multiplies in) transposed to stride L/R, scaled, and rounded
+// once to the plan's element type.  Plan set-up work, never part of a
+// convolution.
+static int to_plan_order(pac_plan_s* pl, const double* in_re, const double* in_im, int nfilters,
+                         void* out_re, void* out_im, double scale, void* stream) {
+  const Schedule& s = pl->main;
+  const long long total = (long long)nfilters * pl->N;
+  if (s.vax.empty()) {
+    if (s.bytes == 8)
+      return be_scale_copy(total, 8, in_re, in_im, out_re, out_im, scale, stream);
+    PAC_TRY(be_round_to_f32(in_re, (float*)out_re, total, stream));
+    return be_round_to_f32(in_im, (float*)out_im, total, stream);
+  }
+  const int logL = s.vax.back().log;
+  const int logR = s.rad.back().back();
+  return be_plan_order(in_re, in_im, out_re, out_im, s.bytes, logL, logR, total >> logL, scale,
+                       stream);
+}
+
 // ---------------------------------------------------------------------------
 // 1D convolution in caller-supplied device scratch (pac_convolve_1d_noalloc).
 // The twiddle tables and the filter spectrum are carved out of `scratch` in
@@ -603,6 +624,7 @@ int conv_in_scratch(void* scratch, size_t scratch_bytes, int logn, int batch, co
   if (st == PAC_SUCCESS)
     st = run_transform(&pl, pl.main, PAC_OP_AT, 1, h_re, h_im, hre, him, 1.0 / (double)pl.N, 1,
                        stream);
+  if (st == PAC_SUCCESS) st = to_plan_order(&pl, hre, him, 1, hre, him, 1.0, stream);
   if (st == PAC_SUCCESS) st = run_conv(&pl, x_re, x_im, hre, him, 0, y_re, y_im, 1.0, stream);
   // the tables live in the caller's scratch: nothing to free
   pl.main.pool = nullptr;
@@ -700,10 +722,14 @@ PAC_API int pac_filter_spectrum(pac_plan_t plan, const double* h_re, const doubl
     return set_error(PAC_ERROR_INVALID_VALUE, "pac_filter_spectrum: NULL argument");
   if (nfilters != 1 && nfilters != plan->batch)
     return set_error(PAC_ERROR_INVALID_VALUE, "pac_filter_spectrum: nfilters must be 1 or batch");
-  if (plan->form == PAC_FORM_F64)
-    return run_transform(plan, plan->main, PAC_OP_AT, nfilters, h_re, h_im, hhat_re, hhat_im, scale,
-                         1, stream);
-  // F32 form: FP64 transform into a temporary, rounded once
+  if (plan->form == PAC_FORM_F64) {
+    // A^T h in P order straight into hhat, then reordered in place
+    PAC_TRY(run_transform(plan, plan->main, PAC_OP_AT, nfilters, h_re, h_im, hhat_re, hhat_im,
+                          scale, 1, stream));
+    return to_plan_order(plan, (const double*)hhat_re, (const double*)hhat_im, nfilters, hhat_re,
+                         hhat_im, 1.0, stream);
+  }
+  // F32 form: FP64 transform into a temporary, reordered and rounded once
   std::lock_guard<std::mutex> g(plan->ws_mu);
   size_t need = (size_t)nfilters * plan->N * 2 * sizeof(double);
   if (plan->tmp64_bytes < need) {
@@ -718,9 +744,21 @@ PAC_API int pac_filter_spectrum(pac_plan_t plan, const double* h_re, const doubl
   // the FP64 schedule never needs the workspace for A^T
   PAC_TRY(run_transform(plan, *plan->s64, PAC_OP_AT, nfilters, h_re, h_im, tre, tim, scale, 1,
                         stream));
-  PAC_TRY(be_round_to_f32(tre, (float*)hhat_re, (long long)nfilters * plan->N, stream));
-  PAC_TRY(be_round_to_f32(tim, (float*)hhat_im, (long long)nfilters * plan->N, stream));
-  return PAC_SUCCESS;
+  return to_plan_order(plan, tre, tim, nfilters, hhat_re, hhat_im, 1.0, stream);
+}
+
+PAC_API int pac_spectrum_to_plan_order(pac_plan_t plan, const double* p_re, const double* p_im,
+                                       int nfilters, void* hhat_re, void* hhat_im, double scale,
+                                       pac_stream_t stream) {
+  if (!plan || !p_re || !p_im || !hhat_re || !hhat_im)
+    return set_error(PAC_ERROR_INVALID_VALUE, "pac_spectrum_to_plan_order: NULL argument");
+  if (nfilters != 1 && nfilters != plan->batch)
+    return set_error(PAC_ERROR_INVALID_VALUE,
+                     "pac_spectrum_to_plan_order: nfilters must be 1 or batch");
+  if (plan->form != PAC_FORM_F64 && (p_re == hhat_re || p_im == hhat_im))
+    return set_error(PAC_ERROR_INVALID_VALUE,
+                     "pac_spectrum_to_plan_order: in place only for PAC_FORM_F64");
+  return to_plan_order(plan, p_re, p_im, nfilters, hhat_re, hhat_im, scale, stream);
 }
 
 PAC_API int pac_convolve(pac_plan_t plan, const void* x_re, const void* x_im, const void* hhat_re,

@@ -232,11 +232,17 @@ PAC_HD void middle_bf(const PassDesc& d, T* sre, T* sim, int src, int dst, int u
   // wants register s = the value at slot sigma_b(s), i.e. register brev(s).
   Cx<T> y[R];
   const T sc = T(d.scale);
+  // The filter spectrum is in plan order: P_b order of the line with every
+  // block of R positions transposed to stride L/R, i.e. P-order slot
+  // blk*R + t sits at t*(L/R) + blk.  For a fixed register s the threads of
+  // a warp (consecutive blk) then read consecutive addresses.  This pass
+  // always runs on the contiguous innermost factor (element stride 1).
+  const int lq = SP::logL(d) - LR;
   static_for<R>([&](auto ss) {
     constexpr int s = ss.value;
     constexpr int p = brev_c(s, LR);
-    const int e = e0 + drev_c(s, LR, B2);
-    long long hi = (lbase[w] + ((long long)e << d.logS)) & d.h_mask;
+    constexpr int t = drev_c(s, LR, B2);
+    long long hi = (lbase[w] + ((long long)t << lq) + (e0 >> LR)) & d.h_mask;
     Cx<T> hv = Cx<T>{ld_g(hre + hi) * sc, ld_g(him + hi) * sc};
     y[s] = cmul(x[p], hv);
   });

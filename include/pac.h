@@ -97,19 +97,32 @@ PAC_API int pac_plan_create(pac_plan_t* plan, int rank, const int* dims, int bat
 PAC_API int pac_plan_destroy(pac_plan_t plan);
 PAC_API int pac_plan_get_info(pac_plan_t plan, pac_plan_info_t* info);
 
-/* Filter spectrum: hhat = scale * A^T h, P_b order, computed in FP64 and
- * rounded once to the plan's storage type.  h_re/h_im are FP64 device
- * arrays of nfilters problems (1, or the plan's batch); hhat has the plan's
- * element type.  In place (h == hhat) is allowed for PAC_FORM_F64.
- * The reference recomputes this inside every call
- * (convolution.c:45-53); the plan API computes it once. */
+/* Filter spectrum: hhat = scale * A^T h, computed in FP64 and rounded once
+ * to the plan's storage type, stored in the plan's spectrum order: the P_b
+ * (digit-reversed) order of A^T h in which, on the innermost axis, every
+ * block of R consecutive positions (R the radix of the plan's last stage)
+ * is transposed to stride L/R, so that the fused pass of pac_convolve reads
+ * it coalesced.  h_re/h_im are FP64 device arrays of nfilters problems (1,
+ * or the plan's batch); hhat has the plan's element type.  In place
+ * (h == hhat) is allowed for PAC_FORM_F64.  The reference recomputes A^T h
+ * inside every call (convolution.c:45-53); the plan API computes it once.
+ * A^T h in the reference's own order is pac_transform(PAC_OP_AT). */
 PAC_API int pac_filter_spectrum(pac_plan_t plan, const double* h_re, const double* h_im,
                                 int nfilters, void* hhat_re, void* hhat_im, double scale,
                                 pac_stream_t stream);
 
+/* A P_b-order FP64 spectrum (e.g. from pac_transform(PAC_OP_AT), or the
+ * reference's A^T h) to the plan's spectrum order, scaled and rounded once.
+ * In place allowed for PAC_FORM_F64.  Set-up work: the convolution itself
+ * never reorders. */
+PAC_API int pac_spectrum_to_plan_order(pac_plan_t plan, const double* p_re, const double* p_im,
+                                       int nfilters, void* hhat_re, void* hhat_im, double scale,
+                                       pac_stream_t stream);
+
 /* Circular convolution of every problem of the batch:
  *   y = conj(A)[ scale * (A^T x) .* hhat ]
- * hhat from pac_filter_spectrum; hhat_per_problem = 0 applies one filter
+ * hhat in the plan's spectrum order (pac_filter_spectrum,
+ * pac_spectrum_to_plan_order); hhat_per_problem = 0 applies one filter
  * spectrum to every problem, 1 reads one spectrum per problem.  x may alias
  * y.  permutation_avoiding_convolution{,_2d,_3d} (convolution.c:31,
  * convolution_2d.c:35, convolution_3d.c:36) with the filter transform

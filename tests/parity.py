@@ -136,3 +136,35 @@ def fftconv(x, h, axes):
 
 def crel(a, b):
     return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
+
+
+def check_spectrum_orders(L, dims, batch, base, form):
+    """pac_transform(A^T) + pac_spectrum_to_plan_order equals
+    pac_filter_spectrum, and A^T h is P_b F h (the reference's order)."""
+    import ctypes as C
+    dt = np.float64 if form == pac.PAC_FORM_F64 else np.float32
+    g = rng(17)
+    h = g.standard_normal(dims) + 1j * g.standard_normal(dims)
+    d = Dev(L)
+    try:
+        plan = pac.Plan(L, dims, 1, base, form)
+        hr, hi = d.put(np.ascontiguousarray(h.real)), d.put(np.ascontiguousarray(h.imag))
+        a_r, a_i = d.zeros(dims, dt), d.zeros(dims, dt)
+        plan.filter_spectrum(hr, hi, a_r, a_i, scale=0.5)
+        plan64 = pac.Plan(L, dims, 1, base, pac.PAC_FORM_F64)
+        p_r, p_i = d.zeros(dims, np.float64), d.zeros(dims, np.float64)
+        plan64.transform(pac.OP_AT, hr, hi, p_r, p_i)
+        pv = d.get(p_r, dims, np.float64) + 1j * d.get(p_i, dims, np.float64)
+        b_r, b_i = d.zeros(dims, dt), d.zeros(dims, dt)
+        pac.check(L, L.pac_spectrum_to_plan_order(plan.h, p_r, p_i, 1, b_r, b_i, 0.5, None), "reorder")
+        a = d.get(a_r, dims, dt) + 1j * d.get(a_i, dims, dt)
+        b = d.get(b_r, dims, dt) + 1j * d.get(b_i, dims, dt)
+        plan.close()
+        plan64.close()
+    finally:
+        d.free()
+    tol = TOL if form == pac.PAC_FORM_F64 else TOL_F32
+    assert crel(a, b) < tol
+    # plan order is a permutation of P order, which is the reference's
+    assert np.allclose(np.sort_complex(a.ravel()), np.sort_complex(0.5 * pv.ravel()),
+                       rtol=tol, atol=tol * np.abs(pv).max())

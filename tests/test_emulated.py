@@ -150,3 +150,9 @@ def test_standalone_permutation(emu, orc):
     emu.apply_permutation(z.ctypes.data_as(C.POINTER(C.c_double)), n,
                           rho.ctypes.data_as(C.POINTER(C.c_int)))
     assert np.array_equal(z[:, 0], re[rho]) and np.array_equal(z[:, 1], im[rho])
+
+
+@pytest.mark.parametrize("dims,base,form", [((2048,), 2, 0), ((64, 2048), 2, 0), ((4096,), 4, 1),
+                                            ((8 ** 3,), 8, 0), ((16, 16, 16), 2, 1)])
+def test_spectrum_orders(emu, dims, base, form):
+    P.check_spectrum_orders(emu, dims, 1, base, form)

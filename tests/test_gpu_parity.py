@@ -206,3 +206,10 @@ def test_concurrent_callers(lib, orc):
     for t in ts:
         t.join()
     assert not errs, errs
+
+
+@pytest.mark.parametrize("dims,base,form", [((2048,), 2, 0), ((2048, 2048), 2, 0),
+                                            ((2048, 2048), 2, 1), ((4096,), 4, 1),
+                                            ((8 ** 3,), 8, 0), ((16, 16, 16), 2, 1)])
+def test_spectrum_orders(lib, dims, base, form):
+    P.check_spectrum_orders(lib, dims, 1, base, form)
