@@ -159,12 +159,24 @@ def check_spectrum_orders(L, dims, batch, base, form):
         pac.check(L, L.pac_spectrum_to_plan_order(plan.h, p_r, p_i, 1, b_r, b_i, 0.5, None), "reorder")
         a = d.get(a_r, dims, dt) + 1j * d.get(a_i, dims, dt)
         b = d.get(b_r, dims, dt) + 1j * d.get(b_i, dims, dt)
+        # the reorder is a bijection: integer labels (exact in FP32 below
+        # 2^24) come out as a permutation of themselves, real and imaginary
+        # parts moved together
+        n = int(np.prod(dims))
+        lab = np.arange(n, dtype=np.float64).reshape(dims)
+        q_r, q_i = d.put(lab), d.put(-2.0 * lab)
+        pac.check(L, L.pac_spectrum_to_plan_order(plan.h, q_r, q_i, 1, b_r, b_i, 1.0, None), "reorder")
+        lr = d.get(b_r, dims, dt).ravel().astype(np.float64)
+        li = d.get(b_i, dims, dt).ravel().astype(np.float64)
         plan.close()
         plan64.close()
     finally:
         d.free()
     tol = TOL if form == pac.PAC_FORM_F64 else TOL_F32
     assert crel(a, b) < tol
-    # plan order is a permutation of P order, which is the reference's
-    assert np.allclose(np.sort_complex(a.ravel()), np.sort_complex(0.5 * pv.ravel()),
-                       rtol=tol, atol=tol * np.abs(pv).max())
+    assert np.array_equal(np.sort(lr), np.arange(n)) and np.array_equal(li, -2.0 * lr)
+    # plan order is a permutation of P order (the reference's order): the
+    # multiset of spectrum values is the same
+    if form == pac.PAC_FORM_F64:
+        assert np.allclose(np.sort_complex(a.ravel()), np.sort_complex(0.5 * pv.ravel()),
+                           rtol=tol, atol=tol * np.abs(pv).max())
