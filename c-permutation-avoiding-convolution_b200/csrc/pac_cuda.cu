@@ -3,13 +3,15 @@
 // Kernels:
 //   pac_pass_kernel<T, B2>   one pass of the butterfly engine (pac_engine.cuh):
 //                            DIF / DIT / fused convolution, any radix schedule
+//   pac_special_kernel       a pass compiled for one geometry (pac_special.h)
+//   pac_cluster_kernel       a column pass whose tile a CTA cluster shares
 //   fill_*_tw                twiddle tables generated in FP64 with sincospi and
 //                            rounded once to the storage type
 //   pointwise, scale_copy, round_to_f32, permute   small elementwise kernels
 //
 // There is no host fallback: every entry point requires an sm_100 device and
 // fails with PAC_ERROR_NO_DEVICE otherwise.
-#include <cudaTypedefs.h>
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include <stdio.h>
 #include <string.h>
@@ -22,6 +24,8 @@
 #include "pac.h"
 #include "pac_backend.h"
 #include "pac_special.h"
+
+namespace cg = cooperative_groups;
 
 namespace pac {
 
@@ -84,119 +88,38 @@ __global__ void __launch_bounds__(NT, MINB) pac_special_kernel(const PassDesc d)
   pass_body_ct<T, B2, MODE, SIGN, SP, NT, RadsFor<LOGL, B2>>(d, cta, sre, sim, s_lb, s_lb);
 }
 
-// ---------------------------------------------------------------------------
-// TMA column passes
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
-               : "memory");
-}
-__device__ __forceinline__ void fence_barrier_init() {
-  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-               "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-      " selp.u32 %0, 1, 0, p;\n}"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// bounded: gives up after ~2^32 SM cycles (about 2 s) instead of spinning forever
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
-  const long long t0 = clock64();
-  while (!mbar_try_wait(bar, parity)) {
-    if (clock64() - t0 > (1LL << 32)) return false;
-  }
-  return true;
-}
-__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0,
-                                            int c1, int c2) {
-  asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
-      "l"((uint64_t)map), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
-      : "memory");
-}
-__device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, const void* src, int c0, int c1,
-                                             int c2) {
-  asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(
-                   (uint64_t)map),
-               "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(src))
-               : "memory");
-}
-__device__ __forceinline__ void bulk_commit() {
-  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
-}
-__device__ __forceinline__ void bulk_wait_read0() {
-  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
-}
-__device__ __forceinline__ void fence_proxy_async() {
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-
-// A column pass (DIF or DIT) over a tile of W columns x L rows that TMA
-// copies into shared memory and back: one elected thread issues the tensor
-// copies, everyone waits on an mbarrier (bounded), the stages run on the
-// swizzled tile, and the tile is stored by tensor copies.
-template <typename T, int B2, int MODE, int SIGN, int LOGL, int LOGW, int NT, int MINB>
-__global__ void __launch_bounds__(NT, MINB)
-    pac_tma_col_kernel(const PassDesc d, const __grid_constant__ CUtensorMap tin_re,
-                       const __grid_constant__ CUtensorMap tin_im,
-                       const __grid_constant__ CUtensorMap tout_re,
-                       const __grid_constant__ CUtensorMap tout_im) {
-  constexpr int W = 1 << LOGW, L = 1 << LOGL;
-  constexpr int BOXR = tma_boxr(LOGL), NBOX = L / BOXR;
-  static_assert(W * sizeof(T) == 16, "16-byte tensor rows");
-  using SP = TmaShape<LOGL, LOGW, (int)sizeof(T)>;
-  extern __shared__ unsigned char pac_smem_raw[];
-  __shared__ __align__(8) uint64_t bar;
+// A column pass whose tile is shared by a cluster of 2^LOGC CTAs
+// (pac_special.h, PAC_CLUSTER_LIST): CTA `rank` of the cluster holds rows
+// [rank * L/C, (rank + 1) * L/C) of the tile's W columns.  Barriers across
+// the cluster separate the phases of pass_body_cl: the first one also
+// guarantees that every CTA of the cluster runs before any distributed
+// shared-memory access, and in DIT the last one keeps each CTA's tile alive
+// while its peers still read it.
+template <typename T, int B2, int MODE, int SIGN, int LOGL, int LOGW, int LOGC, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) pac_cluster_kernel(const PassDesc d) {
+  constexpr int C = 1 << LOGC, W = 1 << LOGW;
+  constexpr int PITCH = pitch_for((int)sizeof(T), LOGL - LOGC, W);
+  using SP = Shape<LOGL, LOGW, PITCH, 1>;
+  using RS = RadsFor<LOGL, B2>;
+  extern __shared__ __align__(16) unsigned char pac_smem[];
   __shared__ long long s_lb[W];
-  T* sre = reinterpret_cast<T*>(((uintptr_t)pac_smem_raw + 1023) & ~(uintptr_t)1023);
-  T* sim = sre + (size_t)W * L;
-  const long long cta = blockIdx.x;
-  const long long g0 = cta * W;
-  const int i0 = (int)(g0 & ((1LL << d.logS) - 1));
-  const int o = (int)(g0 >> d.logS);
-  if ((int)threadIdx.x < W) s_lb[threadIdx.x] = line_base(d, g0 + threadIdx.x);
-  if (threadIdx.x == 0) {
-    mbar_init(&bar, 1);
-    fence_barrier_init();
+  T* sre = reinterpret_cast<T*>(pac_smem);
+  T* sim = sre + (size_t)W * PITCH;
+  cg::cluster_group cl = cg::this_cluster();
+  ClView<T, C> cv;
+  cv.rank = (int)cl.block_rank();
+#pragma unroll
+  for (int r = 0; r < C; ++r) {
+    cv.re[r] = cl.map_shared_rank(sre, r);
+    cv.im[r] = cl.map_shared_rank(sim, r);
   }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    mbar_arrive_expect_tx(&bar, (uint32_t)(2 * W * L * sizeof(T)));
-    for (int k = 0; k < NBOX; ++k) {
-      tma_load_3d(sre + (size_t)k * BOXR * W, &tin_re, &bar, i0, k * BOXR, o);
-      tma_load_3d(sim + (size_t)k * BOXR * W, &tin_im, &bar, i0, k * BOXR, o);
-    }
-  }
-  if (!mbar_wait_bounded(&bar, 0)) {
-    if (threadIdx.x == 0 && d.status) atomicExch(d.status, PAC_ERROR_TIMEOUT);
-    return;
-  }
-  pass_body_ct<T, B2, MODE, SIGN, SP, NT, RadsFor<LOGL, B2>, true>(d, cta, sre, sim, s_lb, s_lb);
-  // generic-proxy writes of the tile become visible to the tensor copy
-  fence_proxy_async();
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    for (int k = 0; k < NBOX; ++k) {
-      tma_store_3d(&tout_re, sre + (size_t)k * BOXR * W, i0, k * BOXR, o);
-      tma_store_3d(&tout_im, sim + (size_t)k * BOXR * W, i0, k * BOXR, o);
-    }
-    bulk_commit();
-    bulk_wait_read0();  // the tile must outlive the copies that read it
-  }
+  const long long cta = (long long)(blockIdx.x >> LOGC);
+  if ((int)threadIdx.x < W) s_lb[threadIdx.x] = line_base(d, cta * W + threadIdx.x);
+  cl.sync();
+  pass_body_cl<T, B2, MODE, SIGN, SP, NT, RS, LOGC>(d, cta, sre, sim, cv, s_lb, 0);
+  cl.sync();
+  pass_body_cl<T, B2, MODE, SIGN, SP, NT, RS, LOGC>(d, cta, sre, sim, cv, s_lb, 1);
+  if constexpr (MODE == MODE_DIT) cl.sync();
 }
 
 template <typename T>
@@ -532,54 +455,19 @@ static int launch_special(const PassDesc& d, int elem_bytes, int b2, long long g
   return set_error(PAC_ERROR_INTERNAL, "no specialised kernel for a pass marked special");
 }
 
-// cuTensorMapEncodeTiled through the runtime's driver entry point (no -lcuda)
-static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-  static std::once_flag once;
-  std::call_once(once, [] {
-    void* p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
-            cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
-  });
-  return fn;
-}
-
-// 3D view (S columns, L rows, O outer) of a column pass's array; box W x BOXR
-static int col_tensor_map(CUtensorMap* m, const void* base, int esz, const PassDesc& d) {
-  auto enc = tensor_map_encoder();
-  if (!enc) return set_error(PAC_ERROR_CUDA, "cuTensorMapEncodeTiled unavailable");
-  const cuuint64_t S = 1ull << d.logS, L = 1ull << d.logL;
-  cuuint64_t dims[3] = {S, L, (cuuint64_t)(d.nlines >> d.logS)};
-  cuuint64_t strides[2] = {S * esz, S * L * esz};
-  cuuint32_t box[3] = {(cuuint32_t)d.W, (cuuint32_t)tma_boxr(d.logL), 1};
-  cuuint32_t estr[3] = {1, 1, 1};
-  CUresult r = enc(m, esz == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
-                   3, const_cast<void*>(base), dims, strides, box, estr,
-                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
-                   CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) return set_error(PAC_ERROR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
-  return PAC_SUCCESS;
-}
-
-static int launch_tma(const PassDesc& d, int elem_bytes, int b2, long long grid, int threads,
-                      size_t smem, void* stream) {
-  CUtensorMap m[4];
-  PAC_TRY_BE(col_tensor_map(&m[0], d.in_re, elem_bytes, d));
-  PAC_TRY_BE(col_tensor_map(&m[1], d.in_im, elem_bytes, d));
-  PAC_TRY_BE(col_tensor_map(&m[2], d.out_re, elem_bytes, d));
-  PAC_TRY_BE(col_tensor_map(&m[3], d.out_im, elem_bytes, d));
-#define PAC_X(T, BY, B2_, MO, SG, LL, LW, NT_, MB)                                             \
+// A cluster pass: grid = tiles x 2^logC CTAs, launched with a cluster shape
+// of (2^logC, 1, 1), so the CTAs of one tile are consecutive blocks.
+static int launch_cluster(const PassDesc& d, int elem_bytes, int b2, long long grid, int threads,
+                          size_t smem, void* stream) {
+#define PAC_X(T, BY, B2_, MO, SG, LL, LW, LC, NT_, MB)                                         \
   if (elem_bytes == BY && b2 == B2_ && d.mode == MO && d.sign == SG && d.logL == LL &&      \
-      d.W == (1 << LW) && threads == NT_) {                                                 \
+      d.W == (1 << LW) && d.logC == LC && threads == NT_) {                                 \
     static std::mutex mu;                                                                   \
     static std::set<int> configured;                                                        \
-    auto kern = pac_tma_col_kernel<T, B2_, MO, SG, LL, LW, NT_, MB>;                        \
+    auto kern = pac_cluster_kernel<T, B2_, MO, SG, LL, LW, LC, NT_, MB>;                    \
     if (smem > 48 * 1024) {                                                                 \
       int dev = 0;                                                                          \
-      cudaGetDevice(&dev);                                                                  \
+      PAC_CU(cudaGetDevice(&dev), "cudaGetDevice");                                         \
       std::lock_guard<std::mutex> g(mu);                                                    \
       if (!configured.count(dev)) {                                                         \
         PAC_CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,      \
@@ -588,19 +476,32 @@ static int launch_tma(const PassDesc& d, int elem_bytes, int b2, long long grid,
         configured.insert(dev);                                                             \
       }                                                                                     \
     }                                                                                       \
-    kern<<<(unsigned)grid, threads, smem, (cudaStream_t)stream>>>(d, m[0], m[1], m[2], m[3]); \
-    PAC_CU(cudaGetLastError(), "pac_tma_col_kernel launch");                                \
+    if (grid > 0x7fffffffLL || (grid & ((1LL << LC) - 1)) != 0)                             \
+      return set_error(PAC_ERROR_INTERNAL, "cluster pass grid %lld", grid);                 \
+    cudaLaunchConfig_t cfg = {};                                                            \
+    cfg.gridDim = dim3((unsigned)grid);                                                     \
+    cfg.blockDim = dim3((unsigned)threads);                                                 \
+    cfg.dynamicSmemBytes = smem;                                                            \
+    cfg.stream = (cudaStream_t)stream;                                                      \
+    cudaLaunchAttribute at[1];                                                              \
+    at[0].id = cudaLaunchAttributeClusterDimension;                                         \
+    at[0].val.clusterDim.x = 1u << LC;                                                      \
+    at[0].val.clusterDim.y = 1;                                                             \
+    at[0].val.clusterDim.z = 1;                                                             \
+    cfg.attrs = at;                                                                         \
+    cfg.numAttrs = 1;                                                                       \
+    PAC_CU(cudaLaunchKernelEx(&cfg, kern, d), "pac_cluster_kernel launch");                 \
     g_launches.fetch_add(1, std::memory_order_relaxed);                                     \
     return PAC_SUCCESS;                                                                     \
   }
-  PAC_TMA_LIST(PAC_X)
+  PAC_CLUSTER_LIST(PAC_X)
 #undef PAC_X
-  return set_error(PAC_ERROR_INTERNAL, "no TMA kernel for a pass marked tma");
+  return set_error(PAC_ERROR_INTERNAL, "no cluster kernel for a pass marked clustered");
 }
 
 int be_launch_pass(const PassDesc& d, int elem_bytes, int b2, long long grid, int threads,
                    size_t smem, void* stream) {
-  if (d.tma) return launch_tma(d, elem_bytes, b2, grid, threads, smem, stream);
+  if (d.logC > 0) return launch_cluster(d, elem_bytes, b2, grid, threads, smem, stream);
   if (d.spec) {
     bool done = false;
     return launch_special(d, elem_bytes, b2, grid, threads, smem, stream, &done);

@@ -11,7 +11,9 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
 #include <atomic>
+#include <limits>
 #include <vector>
 
 #include "pac.h"
@@ -92,54 +94,49 @@ static void replay_special(const PassDesc& d, long long grid) {
   }
 }
 
-// replay of a TMA column kernel: the tile is copied into the swizzled dense
-// layout the tensor copy writes, transformed in place, and copied back
-template <typename T, int B2, int MODE, int SIGN, int LOGL, int LOGW, int NT>
-static void replay_tma(const PassDesc& d, long long grid) {
-  constexpr int W = 1 << LOGW, L = 1 << LOGL;
-  using SP = TmaShape<LOGL, LOGW, (int)sizeof(T)>;
-  std::vector<T> sm((size_t)2 * W * L);
-  T* sre = sm.data();
-  T* sim = sre + (size_t)W * L;
+// replay of a cluster column kernel: each tile's C CTAs get their own
+// shared-memory image; every phase of pass_body_cl runs for all C ranks
+// before the next one starts, as the cluster barriers order them on the
+// device.  The images start as NaN so that a read of an element no stage
+// wrote shows up in the results.
+template <typename T, int B2, int MODE, int SIGN, int LOGL, int LOGW, int LOGC, int NT>
+static void replay_cluster(const PassDesc& d, long long grid) {
+  constexpr int C = 1 << LOGC, W = 1 << LOGW;
+  constexpr int PITCH = pitch_for((int)sizeof(T), LOGL - LOGC, W);
+  using SP = Shape<LOGL, LOGW, PITCH, 1>;
+  const size_t per = (size_t)2 * W * PITCH;
+  std::vector<T> sm(per * C);
   std::vector<long long> lb(W);
-  const T* ire = (const T*)d.in_re;
-  const T* iim = (const T*)d.in_im;
-  T* ore = (T*)d.out_re;
-  T* oim = (T*)d.out_im;
-  for (long long cta = 0; cta < grid; ++cta) {
+  ClView<T, C> cv;
+  for (int r = 0; r < C; ++r) {
+    cv.re[r] = sm.data() + per * r;
+    cv.im[r] = cv.re[r] + (size_t)W * PITCH;
+  }
+  for (long long cta = 0; cta < (grid >> LOGC); ++cta) {
+    std::fill(sm.begin(), sm.end(), std::numeric_limits<T>::quiet_NaN());
     for (int w = 0; w < W; ++w) lb[w] = line_base(d, cta * W + w);
-    for (int w = 0; w < W; ++w)
-      for (int e = 0; e < L; ++e) {
-        long long gi = lb[w] + ((long long)e << d.logS);
-        int si = SP::template sm<T>(d, w, e);
-        sre[si] = ire[gi];
-        sim[si] = iim[gi];
-      }
-    pass_body_ct<T, B2, MODE, SIGN, SP, NT, RadsFor<LOGL, B2>, true>(d, cta, sre, sim, lb.data(),
-                                                                     lb.data());
-    for (int w = 0; w < W; ++w)
-      for (int e = 0; e < L; ++e) {
-        long long gi = lb[w] + ((long long)e << d.logS);
-        int si = SP::template sm<T>(d, w, e);
-        ore[gi] = sre[si];
-        oim[gi] = sim[si];
+    for (int phase = 0; phase < 2; ++phase)
+      for (int r = 0; r < C; ++r) {
+        cv.rank = r;
+        pass_body_cl<T, B2, MODE, SIGN, SP, NT, RadsFor<LOGL, B2>, LOGC>(
+            d, cta, cv.re[r], cv.im[r], cv, lb.data(), phase);
       }
   }
 }
 
 int be_launch_pass(const PassDesc& d, int elem_bytes, int b2, long long grid, int threads,
                    size_t, void*) {
-  if (d.tma) {
-#define PAC_X(T, BY, B2_, MO, SG, LL, LW, NT_, MB)                                         \
-  if (elem_bytes == BY && b2 == B2_ && d.mode == MO && d.sign == SG && d.logL == LL &&  \
-      d.W == (1 << LW) && threads == NT_) {                                             \
-    replay_tma<T, B2_, MO, SG, LL, LW, NT_>(d, grid);                                   \
-    g_launches++;                                                                       \
-    return PAC_SUCCESS;                                                                 \
+  if (d.logC > 0) {
+#define PAC_X(T, BY, B2_, MO, SG, LL, LW, LC, NT_, MB)                                      \
+  if (elem_bytes == BY && b2 == B2_ && d.mode == MO && d.sign == SG && d.logL == LL &&   \
+      d.W == (1 << LW) && d.logC == LC && threads == NT_) {                              \
+    replay_cluster<T, B2_, MO, SG, LL, LW, LC, NT_>(d, grid);                            \
+    g_launches++;                                                                        \
+    return PAC_SUCCESS;                                                                  \
   }
-    PAC_TMA_LIST(PAC_X)
+    PAC_CLUSTER_LIST(PAC_X)
 #undef PAC_X
-    return set_error(PAC_ERROR_INTERNAL, "no TMA replay for a pass marked tma");
+    return set_error(PAC_ERROR_INTERNAL, "no cluster replay for a pass marked clustered");
   }
   if (d.spec) {
     const int cols = d.logS > 0 ? 1 : 0;

@@ -85,8 +85,9 @@ struct PassDesc {
   int* status;
   // 1: this pass runs the kernel specialised for its geometry (pac_special.h)
   int spec;
-  // 1: the specialised column kernel moves its tile with TMA (pac_special.h)
-  int tma;
+  // > 0: a cluster of 2^logC CTAs shares each tile of this specialised
+  // column pass (pac_special.h, PAC_CLUSTER_LIST)
+  int logC;
 };
 
 // ---------------------------------------------------------------------------

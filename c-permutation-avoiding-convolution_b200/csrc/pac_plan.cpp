@@ -294,23 +294,25 @@ static void apply_special(const Schedule& s, PassSpec& p) {
   PassDesc& d = p.d;
   int logW = 0, nt = 0;
   if (d.nat) return;
-  // column pass with a TMA-moved tile: no final scaling (the tile goes back
-  // to global memory by a tensor copy), W columns within the stride, and
-  // 16-byte aligned tensor rows
-  if (d.logS > 0 && !d.use_scale && getenv("PAC_NO_TMA") == nullptr &&
-      tma_geometry(s.bytes, s.b2, d.mode, d.sign, d.logL, &logW, &nt) && logW <= d.logS &&
-      (d.nlines & ((1LL << logW) - 1)) == 0 &&
-      ((uintptr_t)d.in_re | (uintptr_t)d.in_im | (uintptr_t)d.out_re | (uintptr_t)d.out_im) % 16 == 0) {
-    d.W = 1 << logW;
-    d.logW = logW;
-    d.pitch = 0;
-    d.nthreads = nt;
-    d.spec = 1;
-    d.tma = 1;
-    p.threads = nt;
-    p.grid = d.nlines >> logW;
-    p.smem = (size_t)2 * d.W * d.L * s.bytes + 1024;
-    return;
+  // column pass whose tile a CTA cluster shares (W columns within the
+  // stride, whole tiles), opt-in: PAC_CLUSTER_VARIANT=k picks the k-th
+  // candidate geometry of the cluster list
+  const char* cvar = getenv("PAC_CLUSTER_VARIANT");
+  if (d.logS > 0 && cvar != nullptr) {
+    int logC = 0;
+    if (cluster_geometry(s.bytes, s.b2, d.mode, d.sign, d.logL, &logW, &logC, &nt, atoi(cvar)) &&
+        logW <= d.logS && (d.nlines & ((1LL << logW) - 1)) == 0) {
+      d.W = 1 << logW;
+      d.logW = logW;
+      d.logC = logC;
+      d.pitch = pitch_for(s.bytes, d.logL - logC, d.W);
+      d.nthreads = nt;
+      d.spec = 1;
+      p.threads = nt;
+      p.grid = (d.nlines >> logW) << logC;
+      p.smem = (size_t)2 * d.W * d.pitch * s.bytes;
+      return;
+    }
   }
   const char* var = getenv("PAC_SPECIAL_VARIANT");
   const int variant = var ? atoi(var) : 0;

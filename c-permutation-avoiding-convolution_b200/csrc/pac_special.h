@@ -71,26 +71,39 @@ PAC_HDC int pitch_for(int bytes, int logL, int W) {
 // (a geometry may have several candidates; the first is the default and
 // PAC_SPECIAL_VARIANT=k selects the k-th, for tuning)
 
-// Column passes whose tile is moved by TMA (PassDesc.tma).  Empty: with the
-// 128-byte swizzle the tensor copy pads every box row to 128 bytes in shared
-// memory, so a 16-byte-wide column tile would need 8x its size; a dense
-// (unswizzled) tile makes the innermost stage's accesses 8-way bank
-// conflicted.  No column geometry is served by TMA until a layout is both.
+// Column passes whose tile is shared by a cluster of 2^logC CTAs
+// (PassDesc.logC, pass_body_cl): each CTA holds L / 2^logC rows of the
+// W-column tile, so 32- or 64-byte row pieces fit in ~64 KB of shared
+// memory per CTA and two tiles stay resident per SM.  Opt-in
+// (PAC_CLUSTER_VARIANT=k): on 2048^2 FP64 the 2-CTA tiles (W = 4) ran
+// 57 / 59 us per DIF / DIT pass against 54 / 51 us for the one-CTA tiles,
+// and the 4-CTA tiles (W = 8) 69 / 78 us -- the two CTAs of an SM start
+// together, so they load and compute in step, and the exchange through
+// distributed shared memory and the cluster barriers come on top.
 // fields: element type, bytes, log2 digit base, mode, sign, log2 L, log2 W,
-// threads, min CTAs per SM
-#define PAC_TMA_LIST(X)
+// log2 cluster size, threads, min CTAs per SM
+#define PAC_CLUSTER_LIST(X)                          \
+  X(double, 8, 1, MODE_DIF, -1, 11, 2, 1, 256, 2)    \
+  X(double, 8, 1, MODE_DIT, +1, 11, 2, 1, 256, 2)    \
+  X(float, 4, 1, MODE_DIF, -1, 11, 3, 1, 256, 2)     \
+  X(float, 4, 1, MODE_DIT, +1, 11, 3, 1, 256, 2)     \
+  X(double, 8, 1, MODE_DIF, -1, 11, 3, 2, 256, 2)    \
+  X(double, 8, 1, MODE_DIT, +1, 11, 3, 2, 256, 2)    \
+  X(float, 4, 1, MODE_DIF, -1, 11, 4, 2, 256, 2)     \
+  X(float, 4, 1, MODE_DIT, +1, 11, 4, 2, 256, 2)
 
-// rows of the TMA box (the tensor map's box height; a tile is L / TMA_BOXR boxes)
-PAC_HDC int tma_boxr(int logL) { return logL > 8 ? 256 : (1 << logL); }
-
-inline bool tma_geometry(int bytes, int b2, int mode, int sign, int logL, int* logW, int* nt) {
-#define PAC_X(T, BY, B2_, MO, SG, LL, LW, NT_, MB)                                  \
-  if (bytes == BY && b2 == B2_ && mode == MO && sign == SG && logL == LL) {      \
-    *logW = LW;                                                                  \
-    *nt = NT_;                                                                   \
-    return true;                                                                 \
+inline bool cluster_geometry(int bytes, int b2, int mode, int sign, int logL, int* logW,
+                             int* logC, int* nt, int variant = 0) {
+  int seen = 0;
+#define PAC_X(T, BY, B2_, MO, SG, LL, LW, LC, NT_, MB)                                    \
+  if (bytes == BY && b2 == B2_ && mode == MO && sign == SG && logL == LL &&            \
+      seen++ == variant) {                                                             \
+    *logW = LW;                                                                        \
+    *logC = LC;                                                                        \
+    *nt = NT_;                                                                         \
+    return true;                                                                       \
   }
-  PAC_TMA_LIST(PAC_X)
+  PAC_CLUSTER_LIST(PAC_X)
 #undef PAC_X
   return false;
 }

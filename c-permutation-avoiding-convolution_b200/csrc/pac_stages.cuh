@@ -57,30 +57,6 @@ struct Shape {
 };
 using RtShape = Shape<>;
 
-// Column tile moved by TMA: dense [L][W] tile in the 128-byte swizzled order
-// the tensor copy writes (16-byte chunk index, address bits 4-6, XOR-ed with
-// bits 7-9).  Threads take consecutive lines first in every stage, which
-// makes all stage accesses bank-conflict-free for W * ESZ = 16 bytes.
-template <int LOGL_, int LOGW_, int ESZ>
-struct TmaShape {
-  static constexpr int kLogL = LOGL_;
-  static constexpr int kLogW = LOGW_;
-  static constexpr int kPitch = 0;
-  static constexpr int kCols = 1;
-  static PAC_HD int logL(const PassDesc&) { return LOGL_; }
-  static PAC_HD int logW(const PassDesc&) { return LOGW_; }
-  static PAC_HD int W(const PassDesc&) { return 1 << LOGW_; }
-  static PAC_HD int pitch(const PassDesc&) { return 0; }
-  static PAC_HD bool cols(const PassDesc&) { return true; }
-  static PAC_HD bool wfast(const PassDesc&, bool) { return true; }
-  template <typename T>
-  static PAC_HD int sm(const PassDesc&, int w, int e) {
-    uint32_t b = (uint32_t)((e << LOGW_) + w) * ESZ;
-    b ^= ((b >> 7) & 7u) << 4;
-    return (int)(b / ESZ);
-  }
-};
-
 // butterfly index -> (w, blk, j) for a stage of block 2^logK, radix 2^logR
 template <class SP>
 PAC_HD void bf_coords(const PassDesc& d, int logK, int logR, bool global_facing, int u, int* w,
@@ -450,12 +426,10 @@ struct Rads {
 #define PAC_FOR_BF_CT(n, NT, u) for (int u = 0; u < (n); ++u)
 #endif
 
-// SMEM_IO: the tile is already in shared memory (TMA) and is written back
-// there; the first and last stages then read/write shared memory.
-template <typename T, int B2, int MODE, int SIGN, class SP, int NT, class RS, bool SMEM_IO = false>
+template <typename T, int B2, int MODE, int SIGN, class SP, int NT, class RS>
 PAC_HD void pass_body_ct(const PassDesc& d, long long cta, T* sre, T* sim, const long long* lbi,
                          const long long* lbo) {
-  constexpr int GIO = SMEM_IO ? IO_SMEM : IO_GLOBAL;
+  constexpr int GIO = IO_GLOBAL;
   constexpr int LOGL = SP::kLogL;
   constexpr int LOGW = SP::kLogW;
   static_assert(LOGL >= 0 && LOGW >= 0 && SP::kPitch >= 0 && SP::kCols >= 0, "fixed shape");
@@ -517,6 +491,197 @@ PAC_HD void pass_body_ct(const PassDesc& d, long long cta, T* sre, T* sim, const
             d, cta, sre, sim, LK, d.tw_off[i], IO_SMEM, i == 0 ? GIO : IO_SMEM, u, lbi, lbo);
       }
     });
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Cluster column tiles.  C = 2^LOGC CTAs of a thread-block cluster share one
+// tile of W lines of L = 2^LOGL elements: CTA `rank` keeps elements
+// [rank * Lc, (rank + 1) * Lc) of every line in its shared memory (Lc = L/C).
+// A tile then needs 1/C of the shared memory of a one-CTA tile, and several
+// tiles stay resident per SM, so one tile's global loads overlap another's
+// arithmetic.  Only the outermost stage (block L, radix R0 >= C) has
+// butterflies that span CTAs: in DIF it reads global memory and stores each
+// output into the shared memory of the CTA that owns its position
+// (distributed shared memory); in DIT it reads the owners' shared memory and
+// writes global memory.  Every other stage has blocks of at most
+// L / R0 <= Lc elements, which lie inside one CTA.
+// ---------------------------------------------------------------------------
+template <typename T, int C>
+struct ClView {
+  T* re[C];  // shared-memory tile bases of the cluster's CTAs (generic addresses)
+  T* im[C];
+  int rank;  // this CTA's rank in the cluster
+};
+
+// One butterfly of a cluster tile.  XSM: the outermost stage, whose shared-
+// memory side (DIF store, DIT load) addresses the owner CTA of each element.
+template <typename T, int B2, int R, int SIGN, bool DIF, class SP, int LOGK, int LOGC, bool XSM>
+PAC_HD void stage_cl(const PassDesc& d, long long cta, T* sre, T* sim,
+                     const ClView<T, (1 << LOGC)>& cv, int twoff, int src, int dst, int u,
+                     const long long* lbase) {
+  constexpr int LR = ilog2(R);
+  static_assert(LR % B2 == 0, "radix must be a power of the digit base");
+  constexpr int LOGL = SP::kLogL, LOGW = SP::kLogW, PITCH = SP::kPitch;
+  constexpr int LOGLC = LOGL - LOGC;
+  constexpr int logell = LOGK - LR;
+  constexpr int ell = 1 << logell;
+  constexpr int LBF = LOGLC - LR;  // butterflies per line and CTA (log)
+  static_assert(XSM ? LOGK == LOGL : LOGK <= LOGLC, "only the outermost stage spans CTAs");
+  constexpr int OSH = LOGLC - logell;  // XSM: owner of slot s is s >> OSH
+  // global-facing stages: consecutive threads take consecutive lines
+  // (coalesced rows of W elements); others: consecutive butterflies
+  const bool gf = src == IO_GLOBAL || dst == IO_GLOBAL;
+  int w, v;
+  if (gf) {
+    w = u & ((1 << LOGW) - 1);
+    v = u >> LOGW;
+  } else {
+    v = u & ((1 << LBF) - 1);
+    w = u >> LBF;
+  }
+  v += cv.rank << LBF;
+  const int blk = v >> logell;
+  const int j = v & (ell - 1);
+  const int e0 = (blk << LOGK) + j;
+  const T* ire = (const T*)d.in_re;
+  const T* iim = (const T*)d.in_im;
+  Cx<T> x[R];
+  static_for<R>([&](auto mm) {
+    constexpr int m = mm.value;
+    constexpr int slot = DIF ? m : drev_c(m, LR, B2);
+    const int e = e0 + ell * slot;
+    if (src == IO_GLOBAL) {
+      long long gi = lbase[w] + ((long long)e << d.logS);
+      x[m] = Cx<T>{ld_g(ire + gi), ld_g(iim + gi)};
+    } else if constexpr (XSM) {
+      constexpr int o = slot >> OSH;
+      const int si = w * PITCH + sidx<T>(((slot & ((1 << OSH) - 1)) << logell) + j);
+      x[m] = Cx<T>{cv.re[o][si], cv.im[o][si]};
+    } else {
+      const int si = w * PITCH + sidx<T>(e & ((1 << LOGLC) - 1));
+      x[m] = Cx<T>{sre[si], sim[si]};
+    }
+  });
+  const Cx<T>* tw = (const Cx<T>*)d.tw + twoff + j;
+  const bool twiddle = logell > 0 && j > 0;
+  if constexpr (!DIF) {
+    if (d.tw4 == 2 && logell == 0) {
+      static_for<R>([&](auto mm) {
+        constexpr int slot = drev_c(mm.value, LR, B2);
+        x[mm.value] = ctw(x[mm.value], tw4_value<T, B2, SP>(d, cta, w, e0 + slot), SIGN);
+      });
+    }
+    if (twiddle) {
+      static_for<R - 1>([&](auto ss) {
+        constexpr int s = ss.value + 1;
+        x[s] = ctw(x[s], ld_tw(tw + (s - 1) * ell), SIGN);
+      });
+    }
+  }
+  dft_reg<T, R, SIGN>(x);
+  if constexpr (DIF) {
+    if (twiddle) {
+      static_for<R>([&](auto pp) {
+        constexpr int s = brev_c(pp.value, LR);
+        if constexpr (s > 0) x[pp.value] = ctw(x[pp.value], ld_tw(tw + (s - 1) * ell), SIGN);
+      });
+    }
+    if (d.tw4 == 1 && logell == 0) {
+      static_for<R>([&](auto pp) {
+        constexpr int slot = drev_c(brev_c(pp.value, LR), LR, B2);
+        x[pp.value] = ctw(x[pp.value], tw4_value<T, B2, SP>(d, cta, w, e0 + slot), SIGN);
+      });
+    }
+  }
+  T* ore = (T*)d.out_re;
+  T* oim = (T*)d.out_im;
+  static_for<R>([&](auto pp) {
+    constexpr int p = pp.value;
+    constexpr int slot = DIF ? drev_c(brev_c(p, LR), LR, B2) : brev_c(p, LR);
+    const int e = e0 + ell * slot;
+    Cx<T> val = x[p];
+    if (dst == IO_GLOBAL) {
+      if (d.use_scale) {
+        val.re *= T(d.scale);
+        val.im *= T(d.scale);
+      }
+      long long gi = lbase[w] + ((long long)e << d.logS);
+      ore[gi] = val.re;
+      oim[gi] = val.im;
+    } else if constexpr (XSM) {
+      constexpr int o = slot >> OSH;
+      const int si = w * PITCH + sidx<T>(((slot & ((1 << OSH) - 1)) << logell) + j);
+      cv.re[o][si] = val.re;
+      cv.im[o][si] = val.im;
+    } else {
+      const int si = w * PITCH + sidx<T>(e & ((1 << LOGLC) - 1));
+      sre[si] = val.re;
+      sim[si] = val.im;
+    }
+  });
+}
+
+// Phases of a cluster pass; the caller puts a cluster-wide barrier between
+// consecutive phases (and, for DIT, after the last one: the peers read this
+// CTA's tile in phase 1).
+//   DIF  phase 0: outermost stage, global -> owners' shared memory
+//        phase 1: the other stages, local; the last one writes global memory
+//   DIT  phase 0: every stage but the outermost, local; the first reads global
+//        phase 1: outermost stage, owners' shared memory -> global
+template <typename T, int B2, int MODE, int SIGN, class SP, int NT, class RS, int LOGC>
+PAC_HD void pass_body_cl(const PassDesc& d, long long cta, T* sre, T* sim,
+                         const ClView<T, (1 << LOGC)>& cv, const long long* lb, int phase) {
+  constexpr int LOGL = SP::kLogL;
+  constexpr int LOGW = SP::kLogW;
+  constexpr int LOGLC = LOGL - LOGC;
+  constexpr int n = RS::n;
+  static_assert(MODE == MODE_DIF || MODE == MODE_DIT, "cluster passes are DIF or DIT");
+  static_assert(n >= 2 && RS::v[0] >= LOGC, "the outermost stage must span the cluster");
+  if constexpr (MODE == MODE_DIF) {
+    if (phase == 0) {
+      constexpr int LRr = RS::v[0];
+      constexpr int nbf = 1 << (LOGW + LOGLC - LRr);
+      PAC_FOR_BF_CT(nbf, NT, u) {
+        stage_cl<T, B2, (1 << LRr), SIGN, true, SP, LOGL, LOGC, true>(
+            d, cta, sre, sim, cv, d.tw_off[0], IO_GLOBAL, IO_SMEM, u, lb);
+      }
+    } else {
+      static_for<n - 1>([&](auto ii) {
+        constexpr int i = ii.value + 1;
+        constexpr int LK = RS::logK(LOGL, i);
+        constexpr int LRr = RS::v[i];
+        constexpr int nbf = 1 << (LOGW + LOGLC - LRr);
+        if constexpr (i > 1) PAC_SYNC();
+        PAC_FOR_BF_CT(nbf, NT, u) {
+          stage_cl<T, B2, (1 << LRr), SIGN, true, SP, LK, LOGC, false>(
+              d, cta, sre, sim, cv, d.tw_off[i], IO_SMEM, i == n - 1 ? IO_GLOBAL : IO_SMEM, u,
+              lb);
+        }
+      });
+    }
+  } else {
+    if (phase == 0) {
+      static_for<n - 1>([&](auto kk) {
+        constexpr int k = kk.value;
+        constexpr int i = n - 1 - k;
+        constexpr int LK = RS::logK(LOGL, i);
+        constexpr int LRr = RS::v[i];
+        constexpr int nbf = 1 << (LOGW + LOGLC - LRr);
+        if constexpr (k > 0) PAC_SYNC();
+        PAC_FOR_BF_CT(nbf, NT, u) {
+          stage_cl<T, B2, (1 << LRr), SIGN, false, SP, LK, LOGC, false>(
+              d, cta, sre, sim, cv, d.tw_off[i], k == 0 ? IO_GLOBAL : IO_SMEM, IO_SMEM, u, lb);
+        }
+      });
+    } else {
+      constexpr int LRr = RS::v[0];
+      constexpr int nbf = 1 << (LOGW + LOGLC - LRr);
+      PAC_FOR_BF_CT(nbf, NT, u) {
+        stage_cl<T, B2, (1 << LRr), SIGN, false, SP, LOGL, LOGC, true>(
+            d, cta, sre, sim, cv, d.tw_off[0], IO_SMEM, IO_GLOBAL, u, lb);
+      }
+    }
   }
 }
 

@@ -180,3 +180,25 @@ def check_spectrum_orders(L, dims, batch, base, form):
     if form == pac.PAC_FORM_F64:
         assert np.allclose(np.sort_complex(a.ravel()), np.sort_complex(0.5 * pv.ravel()),
                            rtol=tol, atol=tol * np.abs(pv).max())
+
+
+def check_cluster_variants(L, orc, dims, batch, form, monkeypatch, variant):
+    """Column passes served by CTA-cluster tiles (variant k of the cluster
+    list, or none) give the oracle's results: the convolution, A^T, conj(A)
+    and A."""
+    if variant == "off":
+        monkeypatch.delenv("PAC_CLUSTER_VARIANT", raising=False)
+    else:
+        monkeypatch.setenv("PAC_CLUSTER_VARIANT", variant)
+    g = rng(31)
+    shape = (batch,) + tuple(dims)
+    x = g.standard_normal(shape) + 1j * g.standard_normal(shape)
+    h = g.standard_normal(dims) + 1j * g.standard_normal(dims)
+    tol = TOL if form == pac.PAC_FORM_F64 else TOL_F32
+    y = native_conv(L, dims, batch, 2, form, x, h)
+    assert crel(y, fftconv(x, h[None], tuple(range(1, len(shape))))) < tol
+    for op, oop in ((pac.OP_AT, O.OP_AT), (pac.OP_CONJ_A, O.OP_CONJ), (pac.OP_A, O.OP_A)):
+        t = native_transform(L, dims, batch, 2, pac.PAC_FORM_F64, op, x)
+        for b in range(batch):
+            zr, zi = orc.butterflies(oop, 2, x[b].real, x[b].imag)
+            assert crel(t[b], zr + 1j * zi) < TOL

@@ -156,3 +156,11 @@ def test_standalone_permutation(emu, orc):
                                             ((8 ** 3,), 8, 0), ((16, 16, 16), 2, 1)])
 def test_spectrum_orders(emu, dims, base, form):
     P.check_spectrum_orders(emu, dims, 1, base, form)
+
+
+@pytest.mark.parametrize("variant", ["0", "1", "off"])
+@pytest.mark.parametrize("form", [0, 1])
+def test_cluster_column_tiles(emu, orc, monkeypatch, form, variant):
+    """2048-row column passes on tiles shared by 2- and 4-CTA clusters
+    (each cluster phase replayed for all ranks in turn)."""
+    P.check_cluster_variants(emu, orc, (2048, 32), 2, form, monkeypatch, variant)

@@ -213,3 +213,11 @@ def test_concurrent_callers(lib, orc):
                                             ((8 ** 3,), 8, 0), ((16, 16, 16), 2, 1)])
 def test_spectrum_orders(lib, dims, base, form):
     P.check_spectrum_orders(lib, dims, 1, base, form)
+
+
+@pytest.mark.parametrize("variant", ["0", "1", "off"])
+@pytest.mark.parametrize("form", [0, 1])
+def test_cluster_column_tiles(lib, orc, monkeypatch, form, variant):
+    P.check_cluster_variants(lib, orc, (2048, 32), 2, form, monkeypatch, variant)
+    P.check_cluster_variants(lib, orc, (2048, 256), 1, form, monkeypatch, variant)
+
