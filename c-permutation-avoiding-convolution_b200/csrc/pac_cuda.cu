@@ -12,6 +12,7 @@
 // There is no host fallback: every entry point requires an sm_100 device and
 // fails with PAC_ERROR_NO_DEVICE otherwise.
 #include <cooperative_groups.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 #include <stdio.h>
 #include <string.h>
@@ -120,6 +121,140 @@ __global__ void __launch_bounds__(NT, MINB) pac_cluster_kernel(const PassDesc d)
   cl.sync();
   pass_body_cl<T, B2, MODE, SIGN, SP, NT, RS, LOGC>(d, cta, sre, sim, cv, s_lb, 1);
   if constexpr (MODE == MODE_DIT) cl.sync();
+}
+
+// ---------------------------------------------------------------------------
+// Tensor copies (TMA) and mbarriers for the pipelined column passes
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void fence_barrier_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded: gives up after ~2^31 SM cycles (about a second) instead of
+// spinning forever
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity)) {
+    if (clock64() - t0 > (1LL << 31)) return false;
+  }
+  return true;
+}
+// box {W, BOXR, 1} of a 3D tensor map at (c0, c1, c2) into shared memory;
+// completion counted on bar.  No multicast.
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar,
+                                            int c0, int c1, int c2) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
+      "l"((uint64_t)map), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// A pipelined column pass (ColPipe): persistent CTAs walk the tiles
+// blockIdx.x, blockIdx.x + gridDim.x, ...; thread 0 issues the tensor
+// copies of a CTA's next tile as soon as the current one is in registers.
+// Every wait is bounded: on a timeout all threads leave together (after a
+// CTA-wide vote) and the pass reports PAC_ERROR_TIMEOUT in d.status.
+template <typename T, int B2, int MODE, int SIGN, int LOGL, int LOGW, int NT>
+__global__ void __launch_bounds__(NT, 1)
+    pac_pipe_kernel(const PassDesc d, const __grid_constant__ CUtensorMap tin_re,
+                    const __grid_constant__ CUtensorMap tin_im) {
+  using CP = ColPipe<T, B2, MODE, SIGN, LOGL, LOGW, NT>;
+  constexpr int W = CP::W, L = CP::L, BOXR = CP::BOXR, NS = CP::NS;
+  extern __shared__ unsigned char pac_smem_raw[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ long long s_lb[W];
+  // dense tile (tensor-copy destination, 1024-byte aligned), then the
+  // exchange array
+  T* Are = reinterpret_cast<T*>(((uintptr_t)pac_smem_raw + 1023) & ~(uintptr_t)1023);
+  T* Aim = Are + W * L;
+  T* X = Aim + W * L;
+  const int t = threadIdx.x;
+  const long long ntiles = d.nlines >> LOGW;
+  auto issue = [&](long long tl) {
+    const long long g0 = tl << LOGW;
+    const int i0 = (int)(g0 & ((1LL << d.logS) - 1));
+    const int o = (int)(g0 >> d.logS);
+    mbar_arrive_expect_tx(&bar, (uint32_t)(2 * W * L * sizeof(T)));
+    for (int k = 0; k < L / BOXR; ++k) {
+      tma_load_3d(Are + k * BOXR * W, &tin_re, &bar, i0, k * BOXR, o);
+      tma_load_3d(Aim + k * BOXR * W, &tin_im, &bar, i0, k * BOXR, o);
+    }
+  };
+  if (t == 0) {
+    mbar_init(&bar, 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  long long tile = blockIdx.x;
+  if (t == 0 && tile < ntiles) issue(tile);
+  uint32_t phase = 0;
+  Cx<T> x[CP::TPT];
+  for (; tile < ntiles; tile += gridDim.x) {
+    if (t < W) s_lb[t] = line_base(d, tile * W + t);
+    const bool ok = mbar_wait_bounded(&bar, phase);
+    if (!__syncthreads_and(ok)) {
+      if (t == 0 && d.status) atomicExch(d.status, PAC_ERROR_TIMEOUT);
+      if (!ok) mbar_wait_bounded(&bar, phase);  // copies still in flight
+      break;
+    }
+    phase ^= 1;
+    CP::load_tile(t, Are, Aim, x);
+    __syncthreads();  // the tile is in registers: the buffer may be refilled
+    if (t == 0 && tile + gridDim.x < ntiles) {
+      fence_proxy_async();
+      issue(tile + gridDim.x);
+    }
+    if constexpr (MODE == MODE_DIT) {
+      CP::template xw<-1, 0>(t, X, x);
+      __syncthreads();
+      CP::template xr<-1, 0>(t, X, x);
+      __syncthreads();
+      CP::template xw<-1, 1>(t, X, x);
+      __syncthreads();
+      CP::template xr<-1, 1>(t, X, x);
+    }
+    static_for<NS>([&](auto ss) {
+      constexpr int S = ss.value;
+      if constexpr (S > 0) {
+        __syncthreads();
+        CP::template xw<S - 1, 0>(t, X, x);
+        __syncthreads();
+        CP::template xr<S - 1, 0>(t, X, x);
+        __syncthreads();
+        CP::template xw<S - 1, 1>(t, X, x);
+        __syncthreads();
+        CP::template xr<S - 1, 1>(t, X, x);
+      }
+      CP::template compute<S>(d, tile, t, x);
+    });
+    CP::store(d, t, s_lb, x);
+    __syncthreads();  // s_lb and the exchange array are reused by the next tile
+  }
 }
 
 template <typename T>
@@ -281,6 +416,14 @@ int be_init() {
   });
   if (status != PAC_SUCCESS) return set_error(status, "%s", msg);
   return PAC_SUCCESS;
+}
+
+int be_num_sms() {
+  int dev = 0, n = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n < 1)
+    return 1;
+  return n;
 }
 
 int be_malloc(void** p, size_t bytes) {
@@ -499,8 +642,79 @@ static int launch_cluster(const PassDesc& d, int elem_bytes, int b2, long long g
   return set_error(PAC_ERROR_INTERNAL, "no cluster kernel for a pass marked clustered");
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no -lcuda)
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+  });
+  return fn;
+}
+
+// 3D view (S columns, L rows, O = nlines / S outer) of a column pass's input
+// array; box W x boxr x 1, unswizzled, so a box lands as dense rows of W
+// elements
+static int col_tensor_map(CUtensorMap* m, const void* base, int esz, const PassDesc& d,
+                          int boxr) {
+  auto enc = tensor_map_encoder();
+  if (!enc) return set_error(PAC_ERROR_CUDA, "cuTensorMapEncodeTiled unavailable");
+  const cuuint64_t S = 1ull << d.logS, L = 1ull << d.logL;
+  cuuint64_t dims[3] = {S, L, (cuuint64_t)(d.nlines >> d.logS)};
+  cuuint64_t strides[2] = {S * esz, S * L * esz};
+  cuuint32_t box[3] = {(cuuint32_t)d.W, (cuuint32_t)boxr, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = enc(m, esz == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                   3, const_cast<void*>(base), dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS)
+    return set_error(PAC_ERROR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return PAC_SUCCESS;
+}
+
+static int launch_pipe(const PassDesc& d, int elem_bytes, int b2, long long grid, int threads,
+                       size_t smem, void* stream) {
+#define PAC_X(T, BY, B2_, MO, SG, LL, LW, NT_)                                               \
+  if (elem_bytes == BY && b2 == B2_ && d.mode == MO && d.sign == SG && d.logL == LL &&      \
+      d.W == (1 << LW) && threads == NT_) {                                                 \
+    using CP = ColPipe<T, B2_, MO, SG, LL, LW, NT_>;                                        \
+    static std::mutex mu;                                                                   \
+    static std::set<int> configured;                                                        \
+    auto kern = pac_pipe_kernel<T, B2_, MO, SG, LL, LW, NT_>;                               \
+    CUtensorMap m[2];                                                                       \
+    PAC_TRY_BE(col_tensor_map(&m[0], d.in_re, BY, d, CP::BOXR));                            \
+    PAC_TRY_BE(col_tensor_map(&m[1], d.in_im, BY, d, CP::BOXR));                            \
+    {                                                                                       \
+      int dev = 0;                                                                          \
+      PAC_CU(cudaGetDevice(&dev), "cudaGetDevice");                                         \
+      std::lock_guard<std::mutex> g(mu);                                                    \
+      if (!configured.count(dev)) {                                                         \
+        PAC_CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,      \
+                                    (int)smem),                                             \
+               "cudaFuncSetAttribute");                                                     \
+        configured.insert(dev);                                                             \
+      }                                                                                     \
+    }                                                                                       \
+    if (grid > 0x7fffffffLL) return set_error(PAC_ERROR_SIZE, "pass grid too large");       \
+    kern<<<(unsigned)grid, threads, smem, (cudaStream_t)stream>>>(d, m[0], m[1]);           \
+    PAC_CU(cudaGetLastError(), "pac_pipe_kernel launch");                                   \
+    g_launches.fetch_add(1, std::memory_order_relaxed);                                     \
+    return PAC_SUCCESS;                                                                     \
+  }
+  PAC_PIPE_LIST(PAC_X)
+#undef PAC_X
+  return set_error(PAC_ERROR_INTERNAL, "no pipelined kernel for a pass marked pipelined");
+}
+
 int be_launch_pass(const PassDesc& d, int elem_bytes, int b2, long long grid, int threads,
                    size_t smem, void* stream) {
+  if (d.pipe) return launch_pipe(d, elem_bytes, b2, grid, threads, smem, stream);
   if (d.logC > 0) return launch_cluster(d, elem_bytes, b2, grid, threads, smem, stream);
   if (d.spec) {
     bool done = false;

@@ -26,6 +26,8 @@ int set_error(int status, const char* fmt, ...);
 static std::atomic<long long> g_launches{0};
 
 int be_init() { return PAC_SUCCESS; }
+// a few "SMs", so that persistent kernels replay CTAs that walk several tiles
+int be_num_sms() { return 3; }
 
 int be_malloc(void** p, size_t bytes) {
   *p = aligned_alloc(256, ((bytes ? bytes : 16) + 255) / 256 * 256);
@@ -94,6 +96,58 @@ static void replay_special(const PassDesc& d, long long grid) {
   }
 }
 
+// replay of a pipelined column kernel: the CTAs of the persistent launch
+// visit their tiles in order; the tensor copy becomes a plain copy of the
+// tile into the dense buffer, and each step between two barriers runs for
+// every thread in turn, with the per-thread registers kept in an array.
+// The exchange array starts every tile as NaN.
+template <typename T, int B2, int MODE, int SIGN, int LOGL, int LOGW, int NT>
+static void replay_pipe(const PassDesc& d, long long grid) {
+  using CP = ColPipe<T, B2, MODE, SIGN, LOGL, LOGW, NT>;
+  constexpr int W = CP::W, L = CP::L, NS = CP::NS;
+  struct Regs {
+    Cx<T> v[CP::TPT];
+  };
+  std::vector<T> A((size_t)2 * W * L), X((size_t)W * CP::PITCH);
+  std::vector<Regs> xs(NT);
+  std::vector<long long> lb(W);
+  const T* ire = (const T*)d.in_re;
+  const T* iim = (const T*)d.in_im;
+  const long long ntiles = d.nlines >> LOGW;
+  auto each = [&](auto&& f) {
+    for (int t = 0; t < NT; ++t) f(t, xs[t].v);
+  };
+  for (long long c = 0; c < grid; ++c)
+    for (long long tile = c; tile < ntiles; tile += grid) {
+      for (int w = 0; w < W; ++w) lb[w] = line_base(d, tile * W + w);
+      for (int e = 0; e < L; ++e)
+        for (int w = 0; w < W; ++w) {
+          const long long gi = lb[w] + ((long long)e << d.logS);
+          A[(size_t)e * W + w] = ire[gi];
+          A[(size_t)W * L + (size_t)e * W + w] = iim[gi];
+        }
+      std::fill(X.begin(), X.end(), std::numeric_limits<T>::quiet_NaN());
+      each([&](int t, Cx<T>(&x)[CP::TPT]) { CP::load_tile(t, A.data(), A.data() + W * L, x); });
+      if constexpr (MODE == MODE_DIT) {
+        each([&](int t, Cx<T>(&x)[CP::TPT]) { CP::template xw<-1, 0>(t, X.data(), x); });
+        each([&](int t, Cx<T>(&x)[CP::TPT]) { CP::template xr<-1, 0>(t, X.data(), x); });
+        each([&](int t, Cx<T>(&x)[CP::TPT]) { CP::template xw<-1, 1>(t, X.data(), x); });
+        each([&](int t, Cx<T>(&x)[CP::TPT]) { CP::template xr<-1, 1>(t, X.data(), x); });
+      }
+      static_for<NS>([&](auto ss) {
+        constexpr int S = ss.value;
+        if constexpr (S > 0) {
+          each([&](int t, Cx<T>(&x)[CP::TPT]) { CP::template xw<S - 1, 0>(t, X.data(), x); });
+          each([&](int t, Cx<T>(&x)[CP::TPT]) { CP::template xr<S - 1, 0>(t, X.data(), x); });
+          each([&](int t, Cx<T>(&x)[CP::TPT]) { CP::template xw<S - 1, 1>(t, X.data(), x); });
+          each([&](int t, Cx<T>(&x)[CP::TPT]) { CP::template xr<S - 1, 1>(t, X.data(), x); });
+        }
+        each([&](int t, Cx<T>(&x)[CP::TPT]) { CP::template compute<S>(d, tile, t, x); });
+      });
+      each([&](int t, Cx<T>(&x)[CP::TPT]) { CP::store(d, t, lb.data(), x); });
+    }
+}
+
 // replay of a cluster column kernel: each tile's C CTAs get their own
 // shared-memory image; every phase of pass_body_cl runs for all C ranks
 // before the next one starts, as the cluster barriers order them on the
@@ -126,6 +180,18 @@ static void replay_cluster(const PassDesc& d, long long grid) {
 
 int be_launch_pass(const PassDesc& d, int elem_bytes, int b2, long long grid, int threads,
                    size_t, void*) {
+  if (d.pipe) {
+#define PAC_X(T, BY, B2_, MO, SG, LL, LW, NT_)                                               \
+  if (elem_bytes == BY && b2 == B2_ && d.mode == MO && d.sign == SG && d.logL == LL &&      \
+      d.W == (1 << LW) && threads == NT_) {                                                 \
+    replay_pipe<T, B2_, MO, SG, LL, LW, NT_>(d, grid);                                      \
+    g_launches++;                                                                           \
+    return PAC_SUCCESS;                                                                     \
+  }
+    PAC_PIPE_LIST(PAC_X)
+#undef PAC_X
+    return set_error(PAC_ERROR_INTERNAL, "no pipelined replay for a pass marked pipelined");
+  }
   if (d.logC > 0) {
 #define PAC_X(T, BY, B2_, MO, SG, LL, LW, LC, NT_, MB)                                      \
   if (elem_bytes == BY && b2 == B2_ && d.mode == MO && d.sign == SG && d.logL == LL &&   \

@@ -25,6 +25,8 @@
 
 #include <stdint.h>
 
+#include <utility>
+
 #if defined(__CUDACC__)
 #define PAC_HD __host__ __device__ __forceinline__
 #define PAC_HDC __host__ __device__ constexpr
@@ -88,6 +90,9 @@ struct PassDesc {
   // > 0: a cluster of 2^logC CTAs shares each tile of this specialised
   // column pass (pac_special.h, PAC_CLUSTER_LIST)
   int logC;
+  // 1: pipelined column pass, one persistent CTA per SM with tensor-copy
+  // prefetch of the next tile (pac_special.h, PAC_PIPE_LIST; ColPipe)
+  int pipe;
 };
 
 // ---------------------------------------------------------------------------

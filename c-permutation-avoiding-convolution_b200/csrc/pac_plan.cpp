@@ -314,6 +314,27 @@ static void apply_special(const Schedule& s, PassSpec& p) {
       return;
     }
   }
+  // pipelined column pass, opt-in (PAC_PIPE=1): persistent CTAs, one per
+  // SM, tensor-copy prefetch of the next tile (16-byte aligned input arrays
+  // for the tensor maps)
+  const char* pipe = getenv("PAC_PIPE");
+  if (d.logS > 0 && cvar == nullptr && pipe != nullptr && atoi(pipe) != 0 &&
+      pipe_geometry(s.bytes, s.b2, d.mode, d.sign, d.logL, &logW, &nt) && logW <= d.logS &&
+      (d.nlines & ((1LL << logW) - 1)) == 0 && (d.nlines >> d.logS) < (1LL << 31) &&
+      ((uintptr_t)d.in_re | (uintptr_t)d.in_im) % 16 == 0) {
+    d.W = 1 << logW;
+    d.logW = logW;
+    d.pitch = pitch_for(s.bytes, d.logL, d.W);
+    d.nthreads = nt;
+    d.spec = 1;
+    d.pipe = 1;
+    const long long tiles = d.nlines >> logW;
+    const long long sms = be_num_sms();
+    p.threads = nt;
+    p.grid = tiles < sms ? tiles : sms;
+    p.smem = (size_t)2 * d.W * d.L * s.bytes + (size_t)d.W * d.pitch * s.bytes + 1024;
+    return;
+  }
   const char* var = getenv("PAC_SPECIAL_VARIANT");
   const int variant = var ? atoi(var) : 0;
   if (!special_geometry(s.bytes, s.b2, d.mode, d.sign, d.logL, d.logS > 0 ? 1 : 0, &logW, &nt,

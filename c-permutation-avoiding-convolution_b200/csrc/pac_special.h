@@ -14,43 +14,8 @@
 
 namespace pac {
 
-// Radix schedule of one factor of length 2^lg, digit base 2^b2: the fewest
-// stages of at most 4 bits (radix 16), bits spread evenly, larger stages
-// first; every stage a multiple of b2 bits.
-PAC_HDC int sched_n(int lg, int b2) {
-  if (b2 == 3) return lg / 3;
-  int digits = lg / b2, per = 4 / b2;  // digits per stage at most
-  return (digits + per - 1) / per;
-}
-PAC_HDC int sched_v(int lg, int b2, int i) {
-  if (b2 == 3) return 3;
-  int n = sched_n(lg, b2);
-  int digits = lg / b2;
-  int base = digits / n, extra = digits % n;
-  return (base + (i < extra ? 1 : 0)) * b2;
-}
-
-template <int LG, int B2, class IS>
-struct RadsImpl;
-template <int LG, int B2, int... I>
-struct RadsImpl<LG, B2, std::integer_sequence<int, I...>> {
-  using type = Rads<sched_v(LG, B2, I)...>;
-};
-template <int LG, int B2>
-using RadsFor = typename RadsImpl<LG, B2, std::make_integer_sequence<int, sched_n(LG, B2)>>::type;
-
-// shared-memory line pitch: one pad element every 16 (FP64) / 32 (FP32),
-// then skewed so that the W lines of a column tile start in different banks
-PAC_HDC int pitch_for(int bytes, int logL, int W) {
-  const int L = 1 << logL;
-  const int SH = bytes == 8 ? 4 : 5, NB = bytes == 8 ? 16 : 32;
-  int pitch = L + (L >> SH);
-  if (W > 1) {
-    int want = (NB / (W < NB ? W : NB)) % NB;
-    pitch += ((want - pitch % NB) % NB + NB) % NB;
-  }
-  return pitch;
-}
+// (the radix schedules sched_n / sched_v / RadsFor and the line pitch
+// pitch_for are defined with the stage engine, pac_stages.cuh)
 
 // fields: element type, bytes, log2 digit base, mode, sign (DIF/DIT), log2 L,
 // column tile (element stride > 1), log2 W, threads, min CTAs per SM
@@ -91,6 +56,35 @@ PAC_HDC int pitch_for(int bytes, int logL, int W) {
   X(double, 8, 1, MODE_DIT, +1, 11, 3, 2, 256, 2)    \
   X(float, 4, 1, MODE_DIF, -1, 11, 4, 2, 256, 2)     \
   X(float, 4, 1, MODE_DIT, +1, 11, 4, 2, 256, 2)
+
+// Pipelined column passes (PassDesc.pipe, ColPipe): one persistent CTA per
+// SM, the tile in registers, the next tile brought in by tensor copies
+// while the current one computes.  Rows of W elements are 32 bytes, which
+// keeps every tensor-copy x coordinate a multiple of 16 bytes.  Opt-in
+// (PAC_PIPE=1): on 2048^2 the pass takes 57 / 55 us (FP64 DIF / DIT) and
+// 38 / 36 us (FP32) against 54 / 51 and 36 / 33 us for the one-CTA tiles.
+// Taking the loads off the critical path does not help while 16 warps per
+// SM run each tile's stages in lockstep: the SM issues in ~17% of its
+// cycles, waiting at the barriers between stages and on the exchanges.
+// fields: element type, bytes, log2 digit base, mode, sign, log2 L, log2 W,
+// threads
+#define PAC_PIPE_LIST(X)                            \
+  X(double, 8, 1, MODE_DIF, -1, 11, 2, 512)         \
+  X(double, 8, 1, MODE_DIT, +1, 11, 2, 512)         \
+  X(float, 4, 1, MODE_DIF, -1, 11, 3, 512)          \
+  X(float, 4, 1, MODE_DIT, +1, 11, 3, 512)
+
+inline bool pipe_geometry(int bytes, int b2, int mode, int sign, int logL, int* logW, int* nt) {
+#define PAC_X(T, BY, B2_, MO, SG, LL, LW, NT_)                                      \
+  if (bytes == BY && b2 == B2_ && mode == MO && sign == SG && logL == LL) {      \
+    *logW = LW;                                                                  \
+    *nt = NT_;                                                                   \
+    return true;                                                                 \
+  }
+  PAC_PIPE_LIST(PAC_X)
+#undef PAC_X
+  return false;
+}
 
 inline bool cluster_geometry(int bytes, int b2, int mode, int sign, int logL, int* logW,
                              int* logC, int* nt, int variant = 0) {

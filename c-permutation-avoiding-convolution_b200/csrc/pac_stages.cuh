@@ -88,35 +88,16 @@ PAC_HD Cx<T> tw4_value(const PassDesc& d, long long cta, int w, int e) {
   return cmul(ld_tw(lo + (E & ((1u << d.tw4_lolog) - 1))), ld_tw(hi + (E >> d.tw4_lolog)));
 }
 
-// One butterfly.  CLOGK >= 0 fixes the stage's block size at compile time.
-template <typename T, int B2, int R, int SIGN, bool DIF, class SP, int CLOGK>
-PAC_HD void stage_bf(const PassDesc& d, long long cta, T* sre, T* sim, int logK_rt, int twoff,
-                     int src, int dst, int u, const long long* lbase_in,
-                     const long long* lbase_out) {
+// The arithmetic of one radix-R butterfly on registers x: DIT pre-twiddles,
+// the R-point DFT, DIF post-twiddles.  x[m] holds the element at input slot
+// m (DIF: m, DIT: sigma_b(m)); afterwards register p holds output index
+// brev(p).  e0 is the butterfly's first element, j its index in the block,
+// w its line, ell = 2^logell the element stride.
+template <typename T, int B2, int R, int SIGN, bool DIF, class SP>
+PAC_HD void bf_math(const PassDesc& d, long long cta, Cx<T> (&x)[R], int w, int e0, int j,
+                    int logell, int twoff) {
   constexpr int LR = ilog2(R);
-  static_assert(LR % B2 == 0, "radix must be a power of the digit base");
-  const int logK = CLOGK >= 0 ? CLOGK : logK_rt;
-  const int logell = logK - LR;
-  int w, blk, j;
-  bf_coords<SP>(d, logK, LR, src == IO_GLOBAL || dst == IO_GLOBAL, u, &w, &blk, &j);
   const int ell = 1 << logell;
-  const int e0 = (blk << logK) + j;
-  const T* ire = (const T*)d.in_re;
-  const T* iim = (const T*)d.in_im;
-  Cx<T> x[R];
-  // ---- load
-  static_for<R>([&](auto mm) {
-    constexpr int m = mm.value;
-    constexpr int slot = DIF ? m : drev_c(m, LR, B2);
-    const int e = e0 + ell * slot;
-    if (src == IO_GLOBAL) {
-      long long gi = lbase_in[w] + ((long long)e << d.logS);
-      x[m] = Cx<T>{ld_g(ire + gi), ld_g(iim + gi)};
-    } else {
-      int si = SP::template sm<T>(d, w, e);
-      x[m] = Cx<T>{sre[si], sim[si]};
-    }
-  });
   // stage table, s-major: entry (s-1)*ell + j = w_K^{j s}; for one s the
   // threads of a warp read consecutive j (coalesced)
   const Cx<T>* tw = (const Cx<T>*)d.tw + twoff + j;
@@ -153,6 +134,38 @@ PAC_HD void stage_bf(const PassDesc& d, long long cta, T* sre, T* sim, int logK_
       });
     }
   }
+}
+
+// One butterfly.  CLOGK >= 0 fixes the stage's block size at compile time.
+template <typename T, int B2, int R, int SIGN, bool DIF, class SP, int CLOGK>
+PAC_HD void stage_bf(const PassDesc& d, long long cta, T* sre, T* sim, int logK_rt, int twoff,
+                     int src, int dst, int u, const long long* lbase_in,
+                     const long long* lbase_out) {
+  constexpr int LR = ilog2(R);
+  static_assert(LR % B2 == 0, "radix must be a power of the digit base");
+  const int logK = CLOGK >= 0 ? CLOGK : logK_rt;
+  const int logell = logK - LR;
+  int w, blk, j;
+  bf_coords<SP>(d, logK, LR, src == IO_GLOBAL || dst == IO_GLOBAL, u, &w, &blk, &j);
+  const int ell = 1 << logell;
+  const int e0 = (blk << logK) + j;
+  const T* ire = (const T*)d.in_re;
+  const T* iim = (const T*)d.in_im;
+  Cx<T> x[R];
+  // ---- load
+  static_for<R>([&](auto mm) {
+    constexpr int m = mm.value;
+    constexpr int slot = DIF ? m : drev_c(m, LR, B2);
+    const int e = e0 + ell * slot;
+    if (src == IO_GLOBAL) {
+      long long gi = lbase_in[w] + ((long long)e << d.logS);
+      x[m] = Cx<T>{ld_g(ire + gi), ld_g(iim + gi)};
+    } else {
+      int si = SP::template sm<T>(d, w, e);
+      x[m] = Cx<T>{sre[si], sim[si]};
+    }
+  });
+  bf_math<T, B2, R, SIGN, DIF, SP>(d, cta, x, w, e0, j, logell, twoff);
   // ---- store
   T* ore = (T*)d.out_re;
   T* oim = (T*)d.out_im;
@@ -563,37 +576,7 @@ PAC_HD void stage_cl(const PassDesc& d, long long cta, T* sre, T* sim,
       x[m] = Cx<T>{sre[si], sim[si]};
     }
   });
-  const Cx<T>* tw = (const Cx<T>*)d.tw + twoff + j;
-  const bool twiddle = logell > 0 && j > 0;
-  if constexpr (!DIF) {
-    if (d.tw4 == 2 && logell == 0) {
-      static_for<R>([&](auto mm) {
-        constexpr int slot = drev_c(mm.value, LR, B2);
-        x[mm.value] = ctw(x[mm.value], tw4_value<T, B2, SP>(d, cta, w, e0 + slot), SIGN);
-      });
-    }
-    if (twiddle) {
-      static_for<R - 1>([&](auto ss) {
-        constexpr int s = ss.value + 1;
-        x[s] = ctw(x[s], ld_tw(tw + (s - 1) * ell), SIGN);
-      });
-    }
-  }
-  dft_reg<T, R, SIGN>(x);
-  if constexpr (DIF) {
-    if (twiddle) {
-      static_for<R>([&](auto pp) {
-        constexpr int s = brev_c(pp.value, LR);
-        if constexpr (s > 0) x[pp.value] = ctw(x[pp.value], ld_tw(tw + (s - 1) * ell), SIGN);
-      });
-    }
-    if (d.tw4 == 1 && logell == 0) {
-      static_for<R>([&](auto pp) {
-        constexpr int slot = drev_c(brev_c(pp.value, LR), LR, B2);
-        x[pp.value] = ctw(x[pp.value], tw4_value<T, B2, SP>(d, cta, w, e0 + slot), SIGN);
-      });
-    }
-  }
+  bf_math<T, B2, R, SIGN, DIF, SP>(d, cta, x, w, e0, j, logell, twoff);
   T* ore = (T*)d.out_re;
   T* oim = (T*)d.out_im;
   static_for<R>([&](auto pp) {
@@ -684,5 +667,197 @@ PAC_HD void pass_body_cl(const PassDesc& d, long long cta, T* sre, T* sim,
     }
   }
 }
+
+// Radix schedule of one factor of length 2^lg, digit base 2^b2: the fewest
+// stages of at most 4 bits (radix 16), bits spread evenly, larger stages
+// first; every stage a multiple of b2 bits.
+PAC_HDC int sched_n(int lg, int b2) {
+  if (b2 == 3) return lg / 3;
+  int digits = lg / b2, per = 4 / b2;  // digits per stage at most
+  return (digits + per - 1) / per;
+}
+PAC_HDC int sched_v(int lg, int b2, int i) {
+  if (b2 == 3) return 3;
+  int n = sched_n(lg, b2);
+  int digits = lg / b2;
+  int base = digits / n, extra = digits % n;
+  return (base + (i < extra ? 1 : 0)) * b2;
+}
+
+template <int LG, int B2, class IS>
+struct RadsImpl;
+template <int LG, int B2, int... I>
+struct RadsImpl<LG, B2, std::integer_sequence<int, I...>> {
+  using type = Rads<sched_v(LG, B2, I)...>;
+};
+template <int LG, int B2>
+using RadsFor = typename RadsImpl<LG, B2, std::make_integer_sequence<int, sched_n(LG, B2)>>::type;
+
+// shared-memory line pitch: one pad element every 16 (FP64) / 32 (FP32),
+// then skewed so that the W lines of a column tile start in different banks
+PAC_HDC int pitch_for(int bytes, int logL, int W) {
+  const int L = 1 << logL;
+  const int SH = bytes == 8 ? 4 : 5, NB = bytes == 8 ? 16 : 32;
+  int pitch = L + (L >> SH);
+  if (W > 1) {
+    int want = (NB / (W < NB ? W : NB)) % NB;
+    pitch += ((want - pitch % NB) % NB + NB) % NB;
+  }
+  return pitch;
+}
+
+// ---------------------------------------------------------------------------
+// Pipelined column passes.  One CTA per SM walks over the column tiles
+// (W columns x L rows) of a launch; the tile lives in registers, TPT
+// elements per thread.  A tensor copy (TMA) brings the next tile into a
+// dense shared buffer while the current one runs its stages, so the SM keeps
+// HBM reads in flight while it computes -- a one-CTA-per-SM pass that loads
+// through the LSU path alternates between loading and computing instead, and
+// loads in flight are bounded by the L1 left beside a large shared tile.
+// The stages exchange data through one padded shared array, real parts
+// first and then imaginary parts, which needs half the shared memory of a
+// complex tile.  Global stores go out from registers in the last stage.
+//
+// The members below are per-thread steps between two CTA barriers; the
+// device kernel runs them with __syncthreads() in between, the host replay
+// runs each step for every thread in turn.  "Step" s is the s-th stage in
+// the order of execution (DIF: stage s, DIT: stage NS-1-s).
+// ---------------------------------------------------------------------------
+template <typename T, int B2, int MODE, int SIGN, int LOGL, int LOGW, int NT>
+struct ColPipe {
+  static constexpr int L = 1 << LOGL;
+  static constexpr int W = 1 << LOGW;
+  static constexpr int TPT = (W << LOGL) / NT;  // tile elements per thread
+  static constexpr int PITCH = pitch_for((int)sizeof(T), LOGL, W);
+  static constexpr int BOXR = L < 256 ? L : 256;  // rows of one tensor-copy box
+  using SP = Shape<LOGL, LOGW, PITCH, 1>;
+  using RS = RadsFor<LOGL, B2>;
+  static constexpr int NS = RS::n;
+  static constexpr bool DIF = MODE == MODE_DIF;
+  static_assert(MODE == MODE_DIF || MODE == MODE_DIT, "column passes are DIF or DIT");
+  static_assert(TPT * NT == (W << LOGL), "the tile must split evenly over the threads");
+  static_assert(NS >= 2 && L % BOXR == 0, "at least two stages");
+
+  static PAC_HDC int stage_at(int s) { return DIF ? s : NS - 1 - s; }
+  // threads take consecutive lines first (rows of W elements) in the stage
+  // that stores to global memory and in the DIF stage that reads the dense
+  // tensor-copy tile; the exchange-only stages take consecutive butterflies
+  static PAC_HDC bool wfast(int I) { return DIF ? (I == 0 || I == NS - 1) : I == 0; }
+
+  // line w and element e of register K of thread t in stage I, as the
+  // stage's input (IN) or output
+  template <int I, bool IN, int K>
+  static PAC_HD void where(int t, int& w, int& e) {
+    constexpr int LR = RS::v[I], R = 1 << LR;
+    constexpr int LK = RS::logK(LOGL, I), logell = LK - LR;
+    constexpr int LBF = LOGL - LR;
+    constexpr int b = K >> LR, r = K & (R - 1);
+    constexpr int slot = IN ? (DIF ? r : drev_c(r, LR, B2))
+                            : (DIF ? drev_c(brev_c(r, LR), LR, B2) : brev_c(r, LR));
+    const int u = t + b * NT;
+    int v;
+    if constexpr (wfast(I)) {
+      w = u & (W - 1);
+      v = u >> LOGW;
+    } else {
+      v = u & ((1 << LBF) - 1);
+      w = u >> LBF;
+    }
+    const int blk = v >> logell, j = v & ((1 << logell) - 1);
+    e = (blk << LK) + j + (slot << logell);
+  }
+  // positions after step S; S = -1 is the copy order of a DIT tile
+  // (register K of thread t holds element t + K*NT of the dense tile)
+  template <int S, int K>
+  static PAC_HD void after(int t, int& w, int& e) {
+    if constexpr (S < 0) {
+      const int q = t + K * NT;
+      w = q & (W - 1);
+      e = q >> LOGW;
+    } else {
+      where<stage_at(S), false, K>(t, w, e);
+    }
+  }
+
+  // registers from the dense tile A ([e][w], rows of W elements): DIF in
+  // stage 0's input order, DIT in copy order.  A warp reads whole rows.
+  static PAC_HD void load_tile(int t, const T* Are, const T* Aim, Cx<T> (&x)[TPT]) {
+    static_for<TPT>([&](auto kk) {
+      constexpr int K = kk.value;
+      int w, e;
+      if constexpr (DIF) where<0, true, K>(t, w, e);
+      else after<-1, K>(t, w, e);
+      x[K] = Cx<T>{Are[e * W + w], Aim[e * W + w]};
+    });
+  }
+
+  // the butterflies of step S on the registers
+  template <int S>
+  static PAC_HD void compute(const PassDesc& d, long long tile, int t, Cx<T> (&x)[TPT]) {
+    constexpr int I = stage_at(S);
+    constexpr int LR = RS::v[I], R = 1 << LR;
+    constexpr int LK = RS::logK(LOGL, I), logell = LK - LR;
+    constexpr int LBF = LOGL - LR;
+    static_for<TPT / R>([&](auto bb) {
+      constexpr int b = bb.value;
+      const int u = t + b * NT;
+      int w, v;
+      if constexpr (wfast(I)) {
+        w = u & (W - 1);
+        v = u >> LOGW;
+      } else {
+        v = u & ((1 << LBF) - 1);
+        w = u >> LBF;
+      }
+      const int blk = v >> logell, j = v & ((1 << logell) - 1);
+      Cx<T> y[R];
+      static_for<R>([&](auto rr) { y[rr.value] = x[b * R + rr.value]; });
+      bf_math<T, B2, R, SIGN, DIF, SP>(d, tile, y, w, (blk << LK) + j, j, logell, d.tw_off[I]);
+      static_for<R>([&](auto rr) { x[b * R + rr.value] = y[rr.value]; });
+    });
+  }
+
+  // exchange halves: write component C (0 re, 1 im) at the positions after
+  // step S, read it at the input positions of step S + 1
+  template <int S, int C>
+  static PAC_HD void xw(int t, T* X, const Cx<T> (&x)[TPT]) {
+    static_for<TPT>([&](auto kk) {
+      constexpr int K = kk.value;
+      int w, e;
+      after<S, K>(t, w, e);
+      if constexpr (C == 0) X[w * PITCH + sidx<T>(e)] = x[K].re;
+      else X[w * PITCH + sidx<T>(e)] = x[K].im;
+    });
+  }
+  template <int S, int C>
+  static PAC_HD void xr(int t, const T* X, Cx<T> (&x)[TPT]) {
+    static_for<TPT>([&](auto kk) {
+      constexpr int K = kk.value;
+      int w, e;
+      where<stage_at(S + 1), true, K>(t, w, e);
+      if constexpr (C == 0) x[K].re = X[w * PITCH + sidx<T>(e)];
+      else x[K].im = X[w * PITCH + sidx<T>(e)];
+    });
+  }
+
+  // the last step's outputs to global memory (lb: line bases of the tile)
+  static PAC_HD void store(const PassDesc& d, int t, const long long* lb, const Cx<T> (&x)[TPT]) {
+    T* ore = (T*)d.out_re;
+    T* oim = (T*)d.out_im;
+    static_for<TPT>([&](auto kk) {
+      constexpr int K = kk.value;
+      int w, e;
+      after<NS - 1, K>(t, w, e);
+      Cx<T> v = x[K];
+      if (d.use_scale) {
+        v.re *= T(d.scale);
+        v.im *= T(d.scale);
+      }
+      const long long gi = lb[w] + ((long long)e << d.logS);
+      ore[gi] = v.re;
+      oim[gi] = v.im;
+    });
+  }
+};
 
 }  // namespace pac

@@ -182,14 +182,20 @@ def check_spectrum_orders(L, dims, batch, base, form):
                            rtol=tol, atol=tol * np.abs(pv).max())
 
 
-def check_cluster_variants(L, orc, dims, batch, form, monkeypatch, variant):
-    """Column passes served by CTA-cluster tiles (variant k of the cluster
-    list, or none) give the oracle's results: the convolution, A^T, conj(A)
-    and A."""
-    if variant == "off":
-        monkeypatch.delenv("PAC_CLUSTER_VARIANT", raising=False)
-    else:
-        monkeypatch.setenv("PAC_CLUSTER_VARIANT", variant)
+COLUMN_KERNELS = ("pipe", "tile", "cluster0", "cluster1")
+
+
+def check_column_kernels(L, orc, dims, batch, form, monkeypatch, kind):
+    """Column passes served by each column kernel give the oracle's results
+    (the convolution, A^T, conj(A) and A): one-CTA tiles ("tile", the
+    default), the pipelined persistent kernel ("pipe", PAC_PIPE=1), or tiles
+    shared by a CTA cluster ("clusterK", PAC_CLUSTER_VARIANT=K)."""
+    monkeypatch.delenv("PAC_CLUSTER_VARIANT", raising=False)
+    monkeypatch.delenv("PAC_PIPE", raising=False)
+    if kind == "pipe":
+        monkeypatch.setenv("PAC_PIPE", "1")
+    elif kind.startswith("cluster"):
+        monkeypatch.setenv("PAC_CLUSTER_VARIANT", kind[len("cluster"):])
     g = rng(31)
     shape = (batch,) + tuple(dims)
     x = g.standard_normal(shape) + 1j * g.standard_normal(shape)

@@ -158,9 +158,11 @@ def test_spectrum_orders(emu, dims, base, form):
     P.check_spectrum_orders(emu, dims, 1, base, form)
 
 
-@pytest.mark.parametrize("variant", ["0", "1", "off"])
+@pytest.mark.parametrize("kind", P.COLUMN_KERNELS)
 @pytest.mark.parametrize("form", [0, 1])
-def test_cluster_column_tiles(emu, orc, monkeypatch, form, variant):
-    """2048-row column passes on tiles shared by 2- and 4-CTA clusters
+def test_column_kernels(emu, orc, monkeypatch, form, kind):
+    """2048-row column passes through every column kernel: the pipelined
+    persistent one (its CTAs walk several tiles here: the replay backend
+    reports 3 SMs), one-CTA tiles, and tiles shared by 2- and 4-CTA clusters
     (each cluster phase replayed for all ranks in turn)."""
-    P.check_cluster_variants(emu, orc, (2048, 32), 2, form, monkeypatch, variant)
+    P.check_column_kernels(emu, orc, (2048, 32), 2, form, monkeypatch, kind)

@@ -215,9 +215,11 @@ def test_spectrum_orders(lib, dims, base, form):
     P.check_spectrum_orders(lib, dims, 1, base, form)
 
 
-@pytest.mark.parametrize("variant", ["0", "1", "off"])
+@pytest.mark.parametrize("kind", P.COLUMN_KERNELS)
 @pytest.mark.parametrize("form", [0, 1])
-def test_cluster_column_tiles(lib, orc, monkeypatch, form, variant):
-    P.check_cluster_variants(lib, orc, (2048, 32), 2, form, monkeypatch, variant)
-    P.check_cluster_variants(lib, orc, (2048, 256), 1, form, monkeypatch, variant)
+def test_column_kernels(lib, orc, monkeypatch, form, kind):
+    P.check_column_kernels(lib, orc, (2048, 32), 2, form, monkeypatch, kind)
+    P.check_column_kernels(lib, orc, (2048, 256), 1, form, monkeypatch, kind)
+    # more tiles than SMs: persistent CTAs walk several tiles
+    P.check_column_kernels(lib, orc, (2048, 2048), 1, form, monkeypatch, kind)
 
