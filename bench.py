@@ -2,7 +2,7 @@
 """Benchmark of the permutation-avoiding FFT convolution on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--config c3|c1|c2|c4|c4a] [--form f64|f32]
+                    [--config c3|c1|c2|c4|c4a|c5] [--form f64|f32]
 
 A step is one convolution of one batch of the configuration's synthetic
 input.  The default workload is C3: a 2D 2048 x 2048 complex FP64 circular
@@ -53,6 +53,13 @@ CONFIGS = {
     "c4a": dict(dims=(512, 256, 128), batch=1, radix=2,
                 workload="3D 512x256x128 complex circular convolution, 9x9x9 N(0,1/729) "
                          "stencil"),
+    # the batched uneven workload: shapes from workloads.c5_shapes (seed 5)
+    "c5": dict(dims=None, batch=None, radix=2,
+               workload="batched uneven: 4096 1D convolutions, log2 n uniform on 8..20 "
+                        "(rounded), plus 64 2D, log2 of each side uniform on 6..11; complex "
+                        "FP32, x, h ~ N(0,1), h supported on the first 1/16 of every axis; "
+                        "one multi-plan call per step (work-queue levels replayed as a CUDA "
+                        "graph)"),
 }
 
 # DRAM bytes per convolution (sum over its passes) from one ncu capture of
@@ -469,6 +476,251 @@ def run_e2e(args, world, dist):
             "ms_per_call": round(tm * 1e3, 3)}
 
 
+# ---------------------------------------------------------------------------
+# C5: the batched uneven workload through one multi-plan
+# ---------------------------------------------------------------------------
+def _c5_cpu_task(args):
+    """Reference convolutions (radix 2) of the given shapes, one after the
+    other, until `seconds` of busy time.  Returns (elements, busy seconds)."""
+    import ctypes as C
+    shapes, seconds, seed = args
+    libpath, kind = _cpu_lib()
+    L = C.CDLL(libpath)
+    dp = C.POINTER(C.c_double)
+    g = np.random.default_rng(seed)
+    elems, busy = 0, 0.0
+    while busy < seconds or elems == 0:
+        for s in shapes:
+            x = g.standard_normal(s) + 1j * g.standard_normal(s)
+            h = np.zeros(s, np.complex128)
+            sl = tuple(slice(0, max(1, v // 16)) for v in s)
+            h[sl] = g.standard_normal(h[sl].shape) + 1j * g.standard_normal(h[sl].shape)
+            a = [np.ascontiguousarray(v) for v in (x.real, x.imag, h.real, h.imag)]
+            nd = len(s)
+            if kind == "reference":
+                tw = []
+                for n in s:
+                    pr, pi = C.POINTER(dp)(), C.POINTER(dp)()
+                    L.precompute_twiddles_r2(n, C.byref(pr), C.byref(pi))
+                    tw += [pr, pi]
+                f = getattr(L, "permutation_avoiding_convolution" + ("" if nd == 1 else f"_{nd}d"))
+                t0 = time.perf_counter()
+                f(a[0].ctypes.data_as(dp), a[1].ctypes.data_as(dp), *[C.c_int(v) for v in s],
+                  C.c_int(2), *tw, a[2].ctypes.data_as(dp), a[3].ctypes.data_as(dp))
+                busy += time.perf_counter() - t0
+                for ax, v in enumerate(s):  # the reference's own release of its tables
+                    L.free_twiddles(tw[2 * ax], tw[2 * ax + 1], C.c_int(int(v).bit_length() - 1))
+            else:
+                arr = (C.c_int * nd)(*s)
+                L.orc_convolution_nd.argtypes = [C.c_int, C.c_int, dp, dp, C.c_int,
+                                                 C.POINTER(C.c_int), dp, dp]
+                t0 = time.perf_counter()
+                L.orc_convolution_nd(1, 2, a[0].ctypes.data_as(dp), a[1].ctypes.data_as(dp), nd,
+                                     arr, a[2].ctypes.data_as(dp), a[3].ctypes.data_as(dp))
+                busy += time.perf_counter() - t0
+            elems += int(np.prod(s))
+    return elems, busy
+
+
+def c5_cpu_rate(procs, seconds, nsample=64):
+    """The reference's convolution over a seeded sample of the C5 shapes,
+    split over `procs` spawned processes; GElem/s summed over processes."""
+    shapes = W.c5_shapes()
+    g = np.random.default_rng(11)
+    sample = [shapes[i] for i in g.choice(len(shapes), nsample, replace=False)]
+    parts = [sample[i::procs] for i in range(procs)]
+    parts = [p for p in parts if p]
+    with mp.get_context("spawn").Pool(len(parts)) as pool:
+        res = pool.map(_c5_cpu_task, [(p, seconds, 100 + i) for i, p in enumerate(parts)],
+                       chunksize=1)
+    rate = sum(e / b for e, b in res) / 1e9
+    kind = _cpu_lib()[1]
+    return rate, len(parts), kind, sum(e for e, _ in res), sum(b for _, b in res), nsample
+
+
+def _c5_inputs(torch, dev, shapes, offs):
+    """x (FP32) and h (FP64) of every problem, packed, drawn on the device
+    from a fixed seed; h zero outside the first 1/16 of every axis."""
+    n = int(offs[-1])
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(5)
+    x = [torch.randn(n, generator=gen, device=dev, dtype=torch.float32) for _ in range(2)]
+    h = [torch.randn(n, generator=gen, device=dev, dtype=torch.float64) for _ in range(2)]
+    mask = torch.zeros(n, dtype=torch.float64, device=dev)
+    for p, s in enumerate(shapes):
+        o = int(offs[p])
+        view = mask[o:o + int(np.prod(s))].view(s)
+        view[tuple(slice(0, max(1, v // 16)) for v in s)] = 1.0
+    h = [v * mask for v in h]
+    return x, h
+
+
+def run_c5(args, world, dist):
+    import torch
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    L = pac.load()
+    shapes = W.c5_shapes()
+    m = pac.MultiPlan(L, shapes, 2, pac.PAC_FORM_F32)
+    offs = m.offsets
+    n = int(offs[-1])
+    x, h = _c5_inputs(torch, dev, shapes, offs)
+    H = [torch.empty(n, dtype=torch.float32, device=dev) for _ in range(2)]
+    y = [torch.empty(n, dtype=torch.float32, device=dev) for _ in range(2)]
+    stream = torch.cuda.Stream(dev)  # graph capture needs a non-legacy stream
+    sp = stream.cuda_stream
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    m.filter_spectra(h[0].data_ptr(), h[1].data_ptr(), H[0].data_ptr(), H[1].data_ptr(),
+                     stream=sp)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    spectrum_ms = ev0.elapsed_time(ev1)
+
+    def step():
+        m.convolve(x[0].data_ptr(), x[1].data_ptr(), H[0].data_ptr(), H[1].data_ptr(),
+                   y[0].data_ptr(), y[1].data_ptr(), stream=sp)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    info = m.info()
+    if dist is not None:
+        dist.barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    t_wall = time.perf_counter()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    ms = ev0.elapsed_time(ev1)
+    while time.perf_counter() - t_wall < 1.5:
+        step()
+        torch.cuda.synchronize()
+    clocks = sampler.stop()
+    if dist is not None:
+        tt = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    ms_step = ms / args.steps
+    value = world * n / (ms_step * 1e-3) / 1e9
+
+    # accuracy: a seeded sample of problems (the largest 1D and 2D ones
+    # included) against numpy's FP64 FFT convolution
+    g = np.random.default_rng(7)
+    one = [p for p, s in enumerate(shapes) if len(s) == 1]
+    two = [p for p, s in enumerate(shapes) if len(s) == 2]
+    pick = {max(one, key=lambda p: offs[p + 1] - offs[p]),
+            max(two, key=lambda p: offs[p + 1] - offs[p])}
+    pick |= set(int(v) for v in g.choice(len(shapes), 10, replace=False))
+    errs = []
+    for p in sorted(pick):
+        a, b = int(offs[p]), int(offs[p + 1])
+        s = shapes[p]
+        xv = (x[0][a:b].double() + 1j * x[1][a:b].double()).cpu().numpy().reshape(s)
+        hv = (h[0][a:b] + 1j * h[1][a:b]).cpu().numpy().reshape(s)
+        yv = (y[0][a:b].double() + 1j * y[1][a:b].double()).cpu().numpy().reshape(s)
+        axes = tuple(range(len(s)))
+        want = np.fft.ifftn(np.fft.fftn(xv, axes=axes) * np.fft.fftn(hv, axes=axes), axes=axes)
+        errs.append(float(np.linalg.norm((yv - want).ravel()) / np.linalg.norm(want.ravel())))
+
+    peak, peak_kind = read_peaks()
+    alg_bytes = 3 * n * 8  # FP32 complex: read x + read Hhat + write y
+    achieved = alg_bytes / (ms_step * 1e-3) / 1e9
+    out = {"metric": METRIC, "value": round(value, 3), "unit": "GElem/s", "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 4),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+           "data": "synthetic, seeded (torch generator on the device, seed 5; shapes from "
+                   "numpy default_rng seed 5)",
+           "config": {"workload": CONFIGS["c5"]["workload"], "problems": len(shapes),
+                      "shapes": info["nshapes"], "elements": n, "form": "f32",
+                      "digit_base": 2, "levels": info["nlevels"],
+                      "work_items_per_level": info["items"], "cuda_graph": bool(info["graph"]),
+                      "l2": f"inputs larger than L2: {n * 8 / 2**30:.1f} GiB per packed array",
+                      "parallelism": f"replicas x{world}"},
+           "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                        "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+                        "peak_source": "measured, MEASURED_PEAKS.json hbm_gbs"
+                        if peak_kind == "measured" else "fallback 6650 GB/s",
+                        "kernel": f"pac_queue_kernel x{info['nlevels']} (one per level)",
+                        "algorithmic_bytes_per_step": alg_bytes},
+           "gpu_launches": int(info["nlevels"] * args.steps), "clocks": clocks,
+           "filter_spectrum_ms": round(spectrum_ms, 3),
+           "rel_l2_vs_numpy_fp64": max(errs), "sampled_problems": len(errs)}
+
+    # e2e: the same call on pinned host buffers, copies included
+    hx = [torch.empty(n, dtype=torch.float32, pin_memory=True) for _ in range(2)]
+    hy = [torch.empty(n, dtype=torch.float32, pin_memory=True) for _ in range(2)]
+    for a, b in zip(hx, x):
+        a.copy_(b)
+    dx = [torch.empty(n, dtype=torch.float32, device=dev) for _ in range(2)]
+    reps = 3
+    times = []
+    for k in range(reps + 1):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        with torch.cuda.stream(stream):
+            for a, b in zip(dx, hx):
+                a.copy_(b, non_blocking=True)
+            m.convolve(dx[0].data_ptr(), dx[1].data_ptr(), H[0].data_ptr(), H[1].data_ptr(),
+                       dx[0].data_ptr(), dx[1].data_ptr(), stream=sp)
+            for a, b in zip(hy, dx):
+                a.copy_(b, non_blocking=True)
+        stream.synchronize()
+        if k:
+            times.append(time.perf_counter() - t0)
+    tm = sum(times) / len(times)
+    out["e2e"] = {"value": round(world * n / tm / 1e9, 4), "unit": "GElem/s",
+                  "h2d_bytes_per_step": 2 * n * 4, "d2h_bytes_per_step": 2 * n * 4,
+                  "call": "pac_multi_convolve on device copies of pinned host buffers "
+                          f"(H2D + call + D2H), mean of {reps} calls",
+                  "ms_per_call": round(tm * 1e3, 2)}
+    m.close()
+    if not args.no_cpu and world == 1:
+        procs = min(os.cpu_count() or 1, 16)
+        rate, used, kind, el, busy, ns = c5_cpu_rate(procs, 1.5)
+        out["cpu_baseline"] = {
+            "value": round(rate, 6), "unit": "GElem/s", "cores": used, "kind": kind,
+            "sample": f"{ns} C5 shapes drawn with seed 11, convolved by the reference "
+                      f"(radix 2) on {used} processes, {busy:.1f} s of CPU work, "
+                      f"{el} elements"}
+    return out
+
+
+def run_reference_c5(args):
+    procs = max(1, min(os.cpu_count() or 1, 64))
+    k_run = max(1, min(args.steps, 5))
+    rates = []
+    t0 = time.perf_counter()
+    for _ in range(k_run):
+        rate, used, kind, el, busy, ns = c5_cpu_rate(procs, 2.0, nsample=min(4 * procs, 256))
+        rates.append(rate)
+    wall = time.perf_counter() - t0
+    value = statistics.mean(rates)
+    desc = {"value": round(value, 6), "unit": "GElem/s", "cores": used, "kind": kind,
+            "sample": f"{k_run} steps, each {ns} C5 shapes (seed 11) on {used} processes for "
+                      f">= 2 s, the reference's permutation_avoiding_convolution{{,_2d}} "
+                      f"(radix 2)"}
+    return {"metric": METRIC, "value": round(value, 6), "unit": "GElem/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(wall / k_run * 1e3, 2), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic, seeded (numpy default_rng)",
+            "config": {"workload": CONFIGS["c5"]["workload"], "form": "f64 (the reference's)",
+                       "parallelism": "host cores"},
+            "impl": "reference", "cpu_baseline": desc,
+            "e2e": {"value": round(value, 6), "unit": "GElem/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
 def run_reference(args):
     cfg = CONFIGS[args.config]
     procs = max(1, min(os.cpu_count() or 1, 64))
@@ -534,7 +786,8 @@ def main():
 
     if args.impl == "reference":
         if rank == 0:
-            print(json.dumps(run_reference(args)), flush=True)
+            ref = run_reference_c5(args) if args.config == "c5" else run_reference(args)
+            print(json.dumps(ref), flush=True)
         return 0
 
     dist = None
@@ -546,6 +799,14 @@ def main():
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         dist = tdist
+    if args.config == "c5":
+        out = run_c5(args, world, dist)
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        if rank == 0:
+            print(json.dumps(out), flush=True)
+        return 0
     out = run_ours(args, world, dist)
     out["e2e"] = run_e2e(args, world, dist)
     if not args.no_forms and args.form == "f64":

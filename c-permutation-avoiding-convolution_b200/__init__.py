@@ -81,6 +81,12 @@ def _declare(L):
     L.pac_stream_wait_stream.argtypes = [_vp, _vp]
     L.pac_stream_set_l2_persisting.argtypes = [_vp, _vp, sz]
     L.pac_launch_count.restype = ll
+    L.pac_multi_create.argtypes = [C.POINTER(_vp), i, C.POINTER(i), C.POINTER(i), i, i]
+    L.pac_multi_destroy.argtypes = [_vp]
+    L.pac_multi_offsets.argtypes = [_vp, C.POINTER(ll)]
+    L.pac_multi_filter_spectra.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp]
+    L.pac_multi_convolve.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]
+    L.pac_multi_get_info.argtypes = [_vp, C.POINTER(MultiInfo)]
     L.pac_status_string.restype = C.c_char_p
     L.pac_status_string.argtypes = [i]
     L.pac_last_error.restype = C.c_char_p
@@ -234,6 +240,56 @@ def dropin_twiddles(L, r, n):
 # ---------------------------------------------------------------------------
 # native plan API (device pointers)
 # ---------------------------------------------------------------------------
+class MultiInfo(C.Structure):
+    _fields_ = [("nprob", C.c_int), ("nshapes", C.c_int), ("nlevels", C.c_int),
+                ("items", C.c_longlong * 8), ("elements", C.c_longlong), ("graph", C.c_int)]
+
+
+class MultiPlan:
+    """pac.h multi-plan: many convolutions of uneven shapes per call, over
+    packed split arrays (problem p at elements offsets[p]:offsets[p+1])."""
+
+    def __init__(self, L, shapes, digit_base=2, form=PAC_FORM_F32):
+        self.L = L
+        self.h = _vp()
+        n = len(shapes)
+        ranks = (C.c_int * n)(*[len(s) for s in shapes])
+        dims = (C.c_int * (3 * n))(*[v for s in shapes for v in (tuple(s) + (1, 1, 1))[:3]])
+        check(L, L.pac_multi_create(C.byref(self.h), n, ranks, dims, digit_base, form),
+              "pac_multi_create")
+        off = (C.c_longlong * (n + 1))()
+        check(L, L.pac_multi_offsets(self.h, off), "pac_multi_offsets")
+        self.offsets = np.array(off[:], dtype=np.int64)
+        self.shapes = [tuple(s) for s in shapes]
+        self.form = form
+
+    def filter_spectra(self, h_re, h_im, hhat_re, hhat_im, stream=None):
+        check(self.L, self.L.pac_multi_filter_spectra(self.h, h_re, h_im, hhat_re, hhat_im, stream),
+              "pac_multi_filter_spectra")
+
+    def convolve(self, x_re, x_im, hhat_re, hhat_im, y_re, y_im, stream=None):
+        check(self.L, self.L.pac_multi_convolve(self.h, x_re, x_im, hhat_re, hhat_im, y_re, y_im,
+                                                stream), "pac_multi_convolve")
+
+    def info(self):
+        inf = MultiInfo()
+        check(self.L, self.L.pac_multi_get_info(self.h, C.byref(inf)), "pac_multi_get_info")
+        return {"nprob": inf.nprob, "nshapes": inf.nshapes, "nlevels": inf.nlevels,
+                "items": list(inf.items[:inf.nlevels]), "elements": inf.elements,
+                "graph": inf.graph}
+
+    def close(self):
+        if self.h:
+            self.L.pac_multi_destroy(self.h)
+            self.h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class Plan:
     """pac.h plan; device pointers are passed as integers."""
 

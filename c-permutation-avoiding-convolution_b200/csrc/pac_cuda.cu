@@ -89,6 +89,59 @@ __global__ void __launch_bounds__(NT, MINB) pac_special_kernel(const PassDesc d)
   pass_body_ct<T, B2, MODE, SIGN, SP, NT, RadsFor<LOGL, B2>>(d, cta, sre, sim, s_lb, s_lb);
 }
 
+// Persistent CTAs over a device work queue (many passes of different
+// geometry in one launch, pac_multi.cpp): thread 0 takes the next item from
+// the counter and finds its pass by binary search over the item starts; the
+// pass descriptor is copied into shared memory and the CTA runs that pass's
+// CTA `item - starts[k]` with the run-time geometry of pac_pass_kernel.
+template <typename T, int B2>
+__global__ void __launch_bounds__(256) pac_queue_kernel(const PassDesc* __restrict__ descs,
+                                                        const long long* __restrict__ starts,
+                                                        int ndesc, long long total,
+                                                        unsigned long long* counter) {
+  extern __shared__ __align__(16) unsigned char pac_smem[];
+  __shared__ PassDesc sd;
+  __shared__ long long s_lb[128];
+  __shared__ long long s_item;
+  __shared__ int s_k;
+  static_assert(sizeof(PassDesc) % sizeof(int) == 0, "descriptor copy in words");
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const long long it = (long long)atomicAdd(counter, 1ULL);
+      int lo = 0, hi = ndesc - 1;
+      if (it < total) {
+        while (lo < hi) {  // largest k with starts[k] <= it
+          const int mid = (lo + hi + 1) >> 1;
+          if (starts[mid] <= it) lo = mid;
+          else hi = mid - 1;
+        }
+      }
+      s_item = it;
+      s_k = lo;
+    }
+    __syncthreads();
+    const long long it = s_item;
+    if (it >= total) break;
+    const int k = s_k;
+    const int* src = reinterpret_cast<const int*>(descs + k);
+    int* dst = reinterpret_cast<int*>(&sd);
+    for (int i = threadIdx.x; i < (int)(sizeof(PassDesc) / sizeof(int)); i += blockDim.x)
+      dst[i] = src[i];
+    __syncthreads();
+    const long long cta = it - starts[k];
+    T* sre = reinterpret_cast<T*>(pac_smem);
+    T* sim = sre + (size_t)sd.W * sd.pitch;
+    if ((int)threadIdx.x < sd.W) {
+      const long long g = cta * sd.W + threadIdx.x;
+      s_lb[threadIdx.x] = line_base(sd, g);
+      s_lb[64 + threadIdx.x] = s_lb[threadIdx.x];
+    }
+    __syncthreads();
+    pass_body<T, B2>(sd, cta, sre, sim, s_lb, s_lb + 64);
+    __syncthreads();  // sd, s_lb and the tile are reused by the next item
+  }
+}
+
 // A column pass whose tile is shared by a cluster of 2^LOGC CTAs
 // (pac_special.h, PAC_CLUSTER_LIST): CTA `rank` of the cluster holds rows
 // [rank * L/C, (rank + 1) * L/C) of the tile's W columns.  Barriers across
@@ -640,6 +693,110 @@ static int launch_cluster(const PassDesc& d, int elem_bytes, int b2, long long g
   PAC_CLUSTER_LIST(PAC_X)
 #undef PAC_X
   return set_error(PAC_ERROR_INTERNAL, "no cluster kernel for a pass marked clustered");
+}
+
+// ---------------------------------------------------------------------------
+// work-queue launches and graphs (pac_multi.cpp)
+// ---------------------------------------------------------------------------
+template <typename T, int B2>
+static int queue_prepare_t(size_t smem, int* grid_per_sm) {
+  static std::mutex mu;
+  static std::set<int> configured;
+  auto kern = pac_queue_kernel<T, B2>;
+  int dev = 0;
+  PAC_CU(cudaGetDevice(&dev), "cudaGetDevice");
+  {
+    std::lock_guard<std::mutex> g(mu);
+    if (!configured.count(dev)) {
+      int optin = 0;
+      PAC_CU(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev),
+             "cudaDeviceGetAttribute");
+      cudaFuncAttributes fa;
+      PAC_CU(cudaFuncGetAttributes(&fa, kern), "cudaFuncGetAttributes");
+      PAC_CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  optin - (int)fa.sharedSizeBytes),
+             "cudaFuncSetAttribute");
+      configured.insert(dev);
+    }
+  }
+  if (grid_per_sm) {
+    int nb = 0;
+    PAC_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, 256, smem),
+           "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    if (nb < 1) return set_error(PAC_ERROR_SIZE, "work-queue pass needs %zu bytes of shared memory", smem);
+    *grid_per_sm = nb;
+  }
+  return PAC_SUCCESS;
+}
+
+static int queue_prepare(int elem_bytes, int b2, size_t smem, int* grid_per_sm) {
+  if (elem_bytes == 8) {
+    if (b2 == 1) return queue_prepare_t<double, 1>(smem, grid_per_sm);
+    if (b2 == 2) return queue_prepare_t<double, 2>(smem, grid_per_sm);
+    return queue_prepare_t<double, 3>(smem, grid_per_sm);
+  }
+  if (b2 == 1) return queue_prepare_t<float, 1>(smem, grid_per_sm);
+  if (b2 == 2) return queue_prepare_t<float, 2>(smem, grid_per_sm);
+  return queue_prepare_t<float, 3>(smem, grid_per_sm);
+}
+
+int be_queue_prepare(int elem_bytes, int b2, size_t smem) {
+  return queue_prepare(elem_bytes, b2, smem, nullptr);
+}
+
+int be_launch_queue(const PassDesc* descs, const long long* starts, int ndesc, long long total,
+                    unsigned long long* counter, int elem_bytes, int b2, size_t smem,
+                    void* stream) {
+  if (total <= 0) return PAC_SUCCESS;
+  int per_sm = 0;
+  PAC_TRY_BE(queue_prepare(elem_bytes, b2, smem, &per_sm));
+  long long grid = (long long)per_sm * be_num_sms();
+  if (grid > total) grid = total;
+  cudaStream_t s = (cudaStream_t)stream;
+#define PAC_Q(T, B)                                                                        \
+  pac_queue_kernel<T, B><<<(unsigned)grid, 256, smem, s>>>(descs, starts, ndesc, total, counter)
+  if (elem_bytes == 8) {
+    if (b2 == 1) PAC_Q(double, 1);
+    else if (b2 == 2) PAC_Q(double, 2);
+    else PAC_Q(double, 3);
+  } else {
+    if (b2 == 1) PAC_Q(float, 1);
+    else if (b2 == 2) PAC_Q(float, 2);
+    else PAC_Q(float, 3);
+  }
+#undef PAC_Q
+  PAC_CU(cudaGetLastError(), "pac_queue_kernel launch");
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return PAC_SUCCESS;
+}
+
+int be_graph_supported() { return 1; }
+
+int be_graph_begin(void* stream) {
+  PAC_CU(cudaStreamBeginCapture((cudaStream_t)stream, cudaStreamCaptureModeThreadLocal),
+         "cudaStreamBeginCapture");
+  return PAC_SUCCESS;
+}
+
+int be_graph_end(void* stream, void** exec) {
+  cudaGraph_t g = nullptr;
+  PAC_CU(cudaStreamEndCapture((cudaStream_t)stream, &g), "cudaStreamEndCapture");
+  cudaGraphExec_t e = nullptr;
+  cudaError_t err = cudaGraphInstantiate(&e, g, 0);
+  cudaGraphDestroy(g);
+  if (err != cudaSuccess) return cuda_fail(err, "cudaGraphInstantiate");
+  *exec = (void*)e;
+  return PAC_SUCCESS;
+}
+
+int be_graph_launch(void* exec, void* stream) {
+  PAC_CU(cudaGraphLaunch((cudaGraphExec_t)exec, (cudaStream_t)stream), "cudaGraphLaunch");
+  return PAC_SUCCESS;
+}
+
+int be_graph_destroy(void* exec) {
+  if (exec) PAC_CU(cudaGraphExecDestroy((cudaGraphExec_t)exec), "cudaGraphExecDestroy");
+  return PAC_SUCCESS;
 }
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no -lcuda)

@@ -384,4 +384,50 @@ int be_permute(long long n, const int* rho, double* re, double* im, void*) {
 
 long long be_launch_count() { return g_launches.load(); }
 
+// work-queue launch: the items in queue order, one CTA each (the queue's
+// order is the one a single persistent CTA would take)
+template <typename T, int B2>
+static void replay_queue(const PassDesc* descs, const long long* starts, int ndesc,
+                         long long total) {
+  std::vector<long long> lb(128);
+  for (long long it = 0; it < total; ++it) {
+    int k = 0;
+    while (k + 1 < ndesc && starts[k + 1] <= it) ++k;
+    const PassDesc& d = descs[k];
+    const long long cta = it - starts[k];
+    std::vector<T> sm((size_t)2 * d.W * d.pitch, std::numeric_limits<T>::quiet_NaN());
+    for (int w = 0; w < d.W; ++w) lb[w] = lb[64 + w] = line_base(d, cta * d.W + w);
+    pass_body<T, B2>(d, cta, sm.data(), sm.data() + (size_t)d.W * d.pitch, lb.data(),
+                     lb.data() + 64);
+  }
+}
+
+int be_queue_prepare(int, int, size_t) { return PAC_SUCCESS; }
+
+int be_launch_queue(const PassDesc* descs, const long long* starts, int ndesc, long long total,
+                    unsigned long long* counter, int elem_bytes, int b2, size_t, void*) {
+  if (elem_bytes == 8) {
+    if (b2 == 1) replay_queue<double, 1>(descs, starts, ndesc, total);
+    else if (b2 == 2) replay_queue<double, 2>(descs, starts, ndesc, total);
+    else replay_queue<double, 3>(descs, starts, ndesc, total);
+  } else {
+    if (b2 == 1) replay_queue<float, 1>(descs, starts, ndesc, total);
+    else if (b2 == 2) replay_queue<float, 2>(descs, starts, ndesc, total);
+    else replay_queue<float, 3>(descs, starts, ndesc, total);
+  }
+  if (total > 0) *counter += (unsigned long long)total;
+  g_launches++;
+  return PAC_SUCCESS;
+}
+
+int be_graph_supported() { return 0; }
+int be_graph_begin(void*) { return set_error(PAC_ERROR_INTERNAL, "no graphs in the host replay"); }
+int be_graph_end(void*, void**) {
+  return set_error(PAC_ERROR_INTERNAL, "no graphs in the host replay");
+}
+int be_graph_launch(void*, void*) {
+  return set_error(PAC_ERROR_INTERNAL, "no graphs in the host replay");
+}
+int be_graph_destroy(void*) { return PAC_SUCCESS; }
+
 }  // namespace pac

@@ -1,0 +1,286 @@
+// pac_multi.cpp -- many convolutions of uneven shapes per call (pac.h,
+// pac_multi_*): one plan per distinct shape, every problem's passes grouped
+// into levels, each level one persistent work-queue launch, the levels of a
+// buffer set captured once into a CUDA graph.
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <vector>
+
+#include "pac.h"
+#include "pac_backend.h"
+
+namespace pac {
+int set_error(int status, const char* fmt, ...);
+int plan_conv_descs(pac_plan_s* pl, const void* x_re, const void* x_im, const void* h_re,
+                    const void* h_im, void* y_re, void* y_im, std::vector<PassDesc>& descs,
+                    std::vector<long long>& ctas, std::vector<size_t>& smem);
+int plan_bytes(pac_plan_s* pl);
+}  // namespace pac
+
+using namespace pac;
+
+#define PAC_TRY(expr)                    \
+  do {                                   \
+    int _st = (expr);                    \
+    if (_st != PAC_SUCCESS) return _st;  \
+  } while (0)
+
+namespace {
+
+enum { kMaxLevels = 8 };
+
+struct Level {
+  int ndesc = 0;
+  long long total = 0;  // work items (CTAs)
+  size_t smem = 0;
+  size_t desc_off = 0;   // byte offsets into the device block
+  size_t start_off = 0;
+};
+
+}  // namespace
+
+struct pac_multi_s {
+  int nprob = 0;
+  int bytes = 8;
+  int b2 = 1;
+  std::vector<long long> off;       // nprob + 1
+  std::vector<int> shape_of;        // problem -> plan index
+  std::vector<pac_plan_t> plans;    // one per distinct shape
+  std::vector<long long> nelem;     // per plan: elements of one problem
+  // launch state of the last buffer set
+  std::mutex mu;
+  const void* key[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  bool built = false;
+  std::vector<Level> levels;
+  void* dev = nullptr;  // descriptors, starts and counters of all levels
+  size_t dev_bytes = 0;
+  size_t counter_off = 0;
+  void* graph = nullptr;
+  void* graph_stream = nullptr;
+  ~pac_multi_s() {
+    if (graph) be_graph_destroy(graph);
+    if (dev) be_free(dev);
+    for (pac_plan_t p : plans) pac_plan_destroy(p);
+  }
+};
+
+// Gather every problem's pass list for the buffer set, group the passes into
+// levels, order each level's passes by tile size (largest first: the queue
+// hands out the long CTAs early) and upload descriptors and item starts.
+static int build_levels(pac_multi_s* m, const void* x_re, const void* x_im, const void* h_re,
+                        const void* h_im, void* y_re, void* y_im, void* stream) {
+  struct Item {
+    PassDesc d;
+    long long ctas;
+    size_t smem;
+    long long work;  // elements per CTA
+  };
+  std::vector<std::vector<Item>> lv;
+  const size_t B = (size_t)m->bytes;
+  for (int p = 0; p < m->nprob; ++p) {
+    const size_t o = (size_t)m->off[p] * B;
+    std::vector<PassDesc> descs;
+    std::vector<long long> ctas;
+    std::vector<size_t> smem;
+    PAC_TRY(plan_conv_descs(m->plans[m->shape_of[p]], (const char*)x_re + o,
+                            (const char*)x_im + o, (const char*)h_re + o, (const char*)h_im + o,
+                            (char*)y_re + o, (char*)y_im + o, descs, ctas, smem));
+    if (descs.size() > (size_t)kMaxLevels)
+      return set_error(PAC_ERROR_SIZE, "problem %d needs %zu passes (at most %d)", p,
+                       descs.size(), (int)kMaxLevels);
+    if (lv.size() < descs.size()) lv.resize(descs.size());
+    for (size_t k = 0; k < descs.size(); ++k)
+      lv[k].push_back({descs[k], ctas[k], smem[k], (long long)descs[k].W << descs[k].logL});
+  }
+  m->levels.assign(lv.size(), Level());
+  size_t bytes = 0;
+  for (size_t k = 0; k < lv.size(); ++k) {
+    std::stable_sort(lv[k].begin(), lv[k].end(),
+                     [](const Item& a, const Item& b) { return a.work > b.work; });
+    Level& L = m->levels[k];
+    L.ndesc = (int)lv[k].size();
+    L.desc_off = bytes;
+    bytes += (sizeof(PassDesc) * L.ndesc + 255) / 256 * 256;
+    L.start_off = bytes;
+    bytes += (sizeof(long long) * (L.ndesc + 1) + 255) / 256 * 256;
+  }
+  m->counter_off = bytes;
+  bytes += 256;
+  std::vector<unsigned char> host(bytes, 0);
+  for (size_t k = 0; k < lv.size(); ++k) {
+    Level& L = m->levels[k];
+    PassDesc* d = (PassDesc*)(host.data() + L.desc_off);
+    long long* st = (long long*)(host.data() + L.start_off);
+    long long acc = 0;
+    for (int i = 0; i < L.ndesc; ++i) {
+      d[i] = lv[k][i].d;
+      st[i] = acc;
+      acc += lv[k][i].ctas;
+      L.smem = std::max(L.smem, lv[k][i].smem);
+    }
+    st[L.ndesc] = acc;
+    L.total = acc;
+  }
+  if (m->dev_bytes < bytes) {
+    if (m->dev) PAC_TRY(be_free(m->dev));
+    m->dev = nullptr;
+    m->dev_bytes = 0;
+    PAC_TRY(be_malloc(&m->dev, bytes));
+    m->dev_bytes = bytes;
+  }
+  PAC_TRY(be_memcpy(m->dev, host.data(), bytes, CPY_H2D, stream));
+  // the host staging vector dies here: wait for the copy
+  PAC_TRY(be_stream_sync(stream));
+  for (auto& L : m->levels) PAC_TRY(be_queue_prepare(m->bytes, m->b2, L.smem));
+  return PAC_SUCCESS;
+}
+
+// counters to zero, then one work-queue launch per level
+static int issue_levels(pac_multi_s* m, void* stream) {
+  char* dev = (char*)m->dev;
+  unsigned long long* cnt = (unsigned long long*)(dev + m->counter_off);
+  PAC_TRY(be_memset(cnt, 0, sizeof(unsigned long long) * kMaxLevels, stream));
+  for (size_t k = 0; k < m->levels.size(); ++k) {
+    const Level& L = m->levels[k];
+    PAC_TRY(be_launch_queue((const PassDesc*)(dev + L.desc_off),
+                            (const long long*)(dev + L.start_off), L.ndesc, L.total, cnt + k,
+                            m->bytes, m->b2, L.smem, stream));
+  }
+  return PAC_SUCCESS;
+}
+
+static int ilog_exact(int v, int b2) {
+  if (v < 1 || (v & (v - 1))) return -1;
+  int lg = 0;
+  while ((1 << lg) < v) ++lg;
+  return lg % b2 ? -1 : lg;
+}
+
+extern "C" {
+
+PAC_API int pac_multi_create(pac_multi_t* multi, int nprob, const int* ranks, const int* dims,
+                             int digit_base, int form) {
+  if (!multi || nprob < 1 || !ranks || !dims)
+    return set_error(PAC_ERROR_INVALID_VALUE, "pac_multi_create: invalid arguments");
+  if (digit_base == 0) digit_base = 2;
+  const int b2 = digit_base == 2 ? 1 : digit_base == 4 ? 2 : digit_base == 8 ? 3 : 0;
+  if (!b2)
+    return set_error(PAC_ERROR_UNSUPPORTED_RADIX, "pac_multi_create: digit base %d not in {2,4,8}",
+                     digit_base);
+  std::unique_ptr<pac_multi_s> m(new pac_multi_s());
+  m->nprob = nprob;
+  m->b2 = b2;
+  m->off.assign(nprob + 1, 0);
+  m->shape_of.assign(nprob, 0);
+  std::map<std::vector<int>, int> seen;
+  for (int p = 0; p < nprob; ++p) {
+    const int r = ranks[p];
+    if (r < 1 || r > 3) return set_error(PAC_ERROR_INVALID_VALUE, "problem %d: rank %d", p, r);
+    std::vector<int> key(dims + 3 * p, dims + 3 * p + r);
+    long long n = 1;
+    for (int a = 0; a < r; ++a) {
+      if (ilog_exact(key[a], b2) < 0)
+        return set_error(PAC_ERROR_NOT_POWER, "problem %d: axis %d length %d is not a power of %d",
+                         p, a, key[a], digit_base);
+      n *= key[a];
+    }
+    if (n < 2) return set_error(PAC_ERROR_SIZE, "problem %d has a single element", p);
+    auto it = seen.find(key);
+    if (it == seen.end()) {
+      pac_plan_t pl = nullptr;
+      int st = pac_plan_create(&pl, r, key.data(), 1, digit_base, form);
+      if (st != PAC_SUCCESS) return st;
+      it = seen.emplace(key, (int)m->plans.size()).first;
+      m->plans.push_back(pl);
+      m->nelem.push_back(n);
+    }
+    m->shape_of[p] = it->second;
+    m->off[p + 1] = m->off[p] + n;
+  }
+  m->bytes = plan_bytes(m->plans[0]);
+  *multi = m.release();
+  return PAC_SUCCESS;
+}
+
+PAC_API int pac_multi_destroy(pac_multi_t multi) {
+  delete multi;
+  return PAC_SUCCESS;
+}
+
+PAC_API int pac_multi_offsets(pac_multi_t m, long long* offsets) {
+  if (!m || !offsets) return set_error(PAC_ERROR_INVALID_VALUE, "pac_multi_offsets: NULL");
+  memcpy(offsets, m->off.data(), sizeof(long long) * m->off.size());
+  return PAC_SUCCESS;
+}
+
+PAC_API int pac_multi_filter_spectra(pac_multi_t m, const double* h_re, const double* h_im,
+                                     void* hhat_re, void* hhat_im, pac_stream_t stream) {
+  if (!m || !h_re || !h_im || !hhat_re || !hhat_im)
+    return set_error(PAC_ERROR_INVALID_VALUE, "pac_multi_filter_spectra: NULL");
+  const size_t B = (size_t)m->bytes;
+  for (int p = 0; p < m->nprob; ++p) {
+    const long long o = m->off[p];
+    const int s = m->shape_of[p];
+    PAC_TRY(pac_filter_spectrum(m->plans[s], h_re + o, h_im + o, 1, (char*)hhat_re + o * B,
+                                (char*)hhat_im + o * B, 1.0 / (double)m->nelem[s], stream));
+  }
+  return PAC_SUCCESS;
+}
+
+PAC_API int pac_multi_convolve(pac_multi_t m, const void* x_re, const void* x_im,
+                               const void* hhat_re, const void* hhat_im, void* y_re, void* y_im,
+                               pac_stream_t stream) {
+  if (!m || !x_re || !x_im || !hhat_re || !hhat_im || !y_re || !y_im)
+    return set_error(PAC_ERROR_INVALID_VALUE, "pac_multi_convolve: NULL");
+  std::lock_guard<std::mutex> g(m->mu);
+  const void* key[6] = {x_re, x_im, hhat_re, hhat_im, y_re, y_im};
+  if (!m->built || memcmp(key, m->key, sizeof(key)) != 0) {
+    if (m->graph) {
+      be_graph_destroy(m->graph);
+      m->graph = nullptr;
+    }
+    m->built = false;
+    PAC_TRY(build_levels(m, x_re, x_im, hhat_re, hhat_im, y_re, y_im, stream));
+    memcpy(m->key, key, sizeof(key));
+    m->built = true;
+  }
+  if (stream == nullptr || !be_graph_supported()) return issue_levels(m, stream);
+  if (m->graph && m->graph_stream != stream) {
+    be_graph_destroy(m->graph);
+    m->graph = nullptr;
+  }
+  if (!m->graph) {
+    PAC_TRY(be_graph_begin(stream));
+    int st = issue_levels(m, stream);
+    void* exec = nullptr;
+    int st2 = be_graph_end(stream, &exec);
+    if (st != PAC_SUCCESS) {
+      if (exec) be_graph_destroy(exec);
+      return st;
+    }
+    PAC_TRY(st2);
+    m->graph = exec;
+    m->graph_stream = stream;
+  }
+  return be_graph_launch(m->graph, stream);
+}
+
+PAC_API int pac_multi_get_info(pac_multi_t m, pac_multi_info_t* info) {
+  if (!m || !info) return set_error(PAC_ERROR_INVALID_VALUE, "pac_multi_get_info: NULL");
+  memset(info, 0, sizeof(*info));
+  info->nprob = m->nprob;
+  info->nshapes = (int)m->plans.size();
+  info->nlevels = (int)m->levels.size();
+  for (size_t k = 0; k < m->levels.size() && k < kMaxLevels; ++k)
+    info->items[k] = m->levels[k].total;
+  info->elements = m->off[m->nprob];
+  info->graph = m->graph ? 1 : 0;
+  return PAC_SUCCESS;
+}
+
+}  // extern "C"

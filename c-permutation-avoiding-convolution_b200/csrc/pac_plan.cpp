@@ -487,17 +487,15 @@ static int run_transform(pac_plan_s* pl, const Schedule& s, int op, long long ba
   return PAC_SUCCESS;
 }
 
-static int run_conv(pac_plan_s* pl, const void* x_re, const void* x_im, const void* h_re,
-                    const void* h_im, int per_problem, void* y_re, void* y_im, double scale,
-                    void* stream) {
+// The passes of one convolution call (2m - 1 for m factors): DIF over the
+// outer factors, the fused innermost pass, DIT back; all in place in y.
+static void build_conv_passes(pac_plan_s* pl, const void* x_re, const void* x_im,
+                              const void* h_re, const void* h_im, int per_problem, void* y_re,
+                              void* y_im, double scale, std::vector<PassSpec>& passes) {
   const Schedule& s = pl->main;
   const long long N = pl->N;
   const int m = (int)s.vax.size();
   const long long hmask = per_problem ? -1LL : (N - 1);
-  if (m == 0)
-    return be_pointwise(pl->batch * N, s.bytes, x_re, x_im, h_re, h_im, hmask, y_re, y_im, scale,
-                        stream);
-  std::vector<PassSpec> passes;
   for (int vi = 0; vi < m - 1; ++vi) {
     PassSpec p = make_pass(s, vi, pl->batch, N);
     p.d.mode = MODE_DIF;
@@ -533,8 +531,40 @@ static int run_conv(pac_plan_s* pl, const void* x_re, const void* x_im, const vo
     p.d.out_im = y_im;
     passes.push_back(p);
   }
+}
+
+static int run_conv(pac_plan_s* pl, const void* x_re, const void* x_im, const void* h_re,
+                    const void* h_im, int per_problem, void* y_re, void* y_im, double scale,
+                    void* stream) {
+  const Schedule& s = pl->main;
+  if (s.vax.empty()) {
+    const long long hmask = per_problem ? -1LL : (pl->N - 1);
+    return be_pointwise(pl->batch * pl->N, s.bytes, x_re, x_im, h_re, h_im, hmask, y_re, y_im,
+                        scale, stream);
+  }
+  std::vector<PassSpec> passes;
+  build_conv_passes(pl, x_re, x_im, h_re, h_im, per_problem, y_re, y_im, scale, passes);
   return exec_passes(pl, s, passes, stream);
 }
+
+// For a batch of plans (pac_multi.cpp): the convolution pass descriptors of
+// one problem in the generic kernel's geometry, with their CTA counts and
+// shared-memory sizes.  A problem of one element (no factors) has none.
+int plan_conv_descs(pac_plan_s* pl, const void* x_re, const void* x_im, const void* h_re,
+                    const void* h_im, void* y_re, void* y_im, std::vector<PassDesc>& descs,
+                    std::vector<long long>& ctas, std::vector<size_t>& smem) {
+  std::vector<PassSpec> passes;
+  if (!pl->main.vax.empty())
+    build_conv_passes(pl, x_re, x_im, h_re, h_im, 0, y_re, y_im, 1.0, passes);
+  for (auto& p : passes) {
+    descs.push_back(p.d);
+    ctas.push_back(p.grid);
+    smem.push_back(p.smem);
+  }
+  return PAC_SUCCESS;
+}
+int plan_bytes(pac_plan_s* pl) { return pl->main.bytes; }
+int plan_b2(pac_plan_s* pl) { return pl->b2; }
 
 // P-order FP64 spectrum -> the plan's spectrum storage: every block of R
 // positions (R the last stage radix of the innermost factor, the one the

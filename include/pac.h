@@ -155,6 +155,52 @@ PAC_API int pac_convolve_1d_noalloc(const double* x_re, const double* x_im, cons
                                     const double* h_im, double* y_re, double* y_im, int n,
                                     int batch, pac_stream_t stream);
 
+/* ---- Many convolutions of uneven shapes in one call ----------------------
+ * No counterpart in the reference, which convolves one signal per call
+ * (bench1d_convolution.c loops over sizes).  A multi-plan covers nprob
+ * problems of any mix of ranks and power-of-b shapes (every problem at
+ * least 2 elements); problem p's data occupies elements
+ * [offsets[p], offsets[p+1]) of packed split arrays (pac_multi_offsets),
+ * in the problem's own row-major layout.  Problems of one shape share their
+ * plan and twiddles.
+ *
+ * pac_multi_convolve runs every problem's convolution passes level by level
+ * (level k = the k-th pass of every problem that has one): each level is
+ * ONE persistent launch whose CTAs take work items (pass, tile) from a
+ * device work queue, largest tiles first, so small and large problems share
+ * the GPU.  With a non-NULL stream the levels are captured once into a CUDA
+ * graph per set of buffer addresses and replayed afterwards (the first call
+ * for new addresses captures; later calls launch the graph).  Calls on one
+ * multi-plan are serialised by a lock. */
+typedef struct pac_multi_s* pac_multi_t;
+
+/* ranks[p] in 1..3; dims holds 3 entries per problem (the first ranks[p]
+ * are used). */
+PAC_API int pac_multi_create(pac_multi_t* multi, int nprob, const int* ranks, const int* dims,
+                             int digit_base, int form);
+PAC_API int pac_multi_destroy(pac_multi_t multi);
+/* offsets[0..nprob]: element offset of every problem; offsets[nprob] is the
+ * total element count of one packed array */
+PAC_API int pac_multi_offsets(pac_multi_t multi, long long* offsets);
+/* filter spectra of every problem (packed FP64 h -> packed hhat of the
+ * form's type, each scaled by 1/N of its problem and in its plan's order) */
+PAC_API int pac_multi_filter_spectra(pac_multi_t multi, const double* h_re, const double* h_im,
+                                     void* hhat_re, void* hhat_im, pac_stream_t stream);
+/* y = x (*) h for every problem; x may alias y */
+PAC_API int pac_multi_convolve(pac_multi_t multi, const void* x_re, const void* x_im,
+                               const void* hhat_re, const void* hhat_im, void* y_re, void* y_im,
+                               pac_stream_t stream);
+
+typedef struct {
+  int nprob;
+  int nshapes;            /* distinct shapes (plans) */
+  int nlevels;            /* launches per pac_multi_convolve */
+  long long items[8];     /* work items (CTAs) of each level */
+  long long elements;     /* total elements of one packed array */
+  int graph;              /* 1 once a CUDA graph replays the levels */
+} pac_multi_info_t;
+PAC_API int pac_multi_get_info(pac_multi_t multi, pac_multi_info_t* info);
+
 /* y = scale * x .* h elementwise over n complex FP64 values (the product
  * loop of convolution.c:55-62 on its own; the reference's convolution
  * reduces to it when the radix is not supported). */

@@ -208,3 +208,60 @@ def check_column_kernels(L, orc, dims, batch, form, monkeypatch, kind):
         for b in range(batch):
             zr, zi = orc.butterflies(oop, 2, x[b].real, x[b].imag)
             assert crel(t[b], zr + 1j * zi) < TOL
+
+
+def check_multi(L, shapes, form, stream=False, seed=3):
+    """pac_multi_*: every problem of an uneven batch against numpy's FP64
+    FFT convolution; a second call (the CUDA-graph replay when a stream is
+    given) repeats the first bit for bit."""
+    dt = np.float64 if form == pac.PAC_FORM_F64 else np.float32
+    tol = TOL if form == pac.PAC_FORM_F64 else TOL_F32
+    g = rng(seed)
+    m = pac.MultiPlan(L, shapes, 2, form)
+    off = m.offsets
+    n = int(off[-1])
+    xs, hs = [], []
+    for s in shapes:
+        x = g.standard_normal(s) + 1j * g.standard_normal(s)
+        h = np.zeros(s, np.complex128)
+        sl = tuple(slice(0, max(1, v // 16)) for v in s)
+        h[sl] = g.standard_normal(h[sl].shape) + 1j * g.standard_normal(h[sl].shape)
+        xs.append(x)
+        hs.append(h)
+    xp = np.concatenate([x.ravel() for x in xs])
+    hp = np.concatenate([h.ravel() for h in hs])
+    d = Dev(L)
+    st = None
+    try:
+        if stream:
+            st = C.c_void_p()
+            pac.check(L, L.pac_stream_create(C.byref(st)), "stream")
+        hr, hi = d.put(hp.real.copy()), d.put(hp.imag.copy())
+        Hr, Hi = d.zeros(n, dt), d.zeros(n, dt)
+        m.filter_spectra(hr, hi, Hr, Hi, stream=st)
+        xr, xi = d.put(xp.real.astype(dt)), d.put(xp.imag.astype(dt))
+        yr, yi = d.zeros(n, dt), d.zeros(n, dt)
+        m.convolve(xr, xi, Hr, Hi, yr, yi, stream=st)
+        if st is not None:
+            pac.check(L, L.pac_stream_synchronize(st), "sync")
+        y1 = d.get(yr, n, dt) + 1j * d.get(yi, n, dt)
+        m.convolve(xr, xi, Hr, Hi, yr, yi, stream=st)
+        if st is not None:
+            pac.check(L, L.pac_stream_synchronize(st), "sync")
+        y2 = d.get(yr, n, dt) + 1j * d.get(yi, n, dt)
+        info = m.info()
+    finally:
+        d.free()
+        if st is not None:
+            L.pac_stream_destroy(st)
+        m.close()
+    assert np.array_equal(y1, y2)
+    bad = {}
+    for p, s in enumerate(shapes):
+        y = y1[off[p]:off[p + 1]].reshape(s)
+        z = fftconv(xs[p], hs[p], tuple(range(len(s))))
+        e = crel(y, z)
+        if not e < tol:
+            bad[(p, s)] = e
+    assert not bad, bad
+    return info

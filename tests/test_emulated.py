@@ -166,3 +166,15 @@ def test_column_kernels(emu, orc, monkeypatch, form, kind):
     reports 3 SMs), one-CTA tiles, and tiles shared by 2- and 4-CTA clusters
     (each cluster phase replayed for all ranks in turn)."""
     P.check_column_kernels(emu, orc, (2048, 32), 2, form, monkeypatch, kind)
+
+
+@pytest.mark.parametrize("form", [0, 1])
+def test_multi_uneven_batch(emu, form):
+    """Many convolutions of uneven 1D/2D/3D shapes through the work-queue
+    levels (replayed item by item)."""
+    shapes = [(256,), (1024,), (2 ** 14,), (4096,), (64, 32), (16, 16, 16), (2,), (2048,),
+              (32, 64), (256,), (8192, 2)]
+    info = P.check_multi(emu, shapes, form)
+    assert info["nprob"] == len(shapes) and info["nshapes"] == len(set(shapes))
+    # the 3D shape has three factors: 5 passes, the deepest level count
+    assert info["nlevels"] == 5 and info["graph"] == 0

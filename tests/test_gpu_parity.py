@@ -223,3 +223,14 @@ def test_column_kernels(lib, orc, monkeypatch, form, kind):
     # more tiles than SMs: persistent CTAs walk several tiles
     P.check_column_kernels(lib, orc, (2048, 2048), 1, form, monkeypatch, kind)
 
+
+
+@pytest.mark.parametrize("form", [0, 1])
+@pytest.mark.parametrize("stream", [False, True])
+def test_multi_uneven_batch(lib, form, stream):
+    """Uneven batch through one persistent work-queue launch per level; with
+    a stream the levels are captured into a CUDA graph and replayed."""
+    W5 = W.c5_shapes(48, 6, seed=9)
+    shapes = W5 + [(2 ** 20,), (2048, 512), (16, 16, 16), (2,), (128, 4, 64)]
+    info = P.check_multi(lib, shapes, form, stream=stream)
+    assert info["graph"] == (1 if stream else 0)
