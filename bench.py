@@ -613,6 +613,15 @@ def run_c5(args, world, dist):
     ms_step = ms / args.steps
     value = world * n / (ms_step * 1e-3) / 1e9
 
+    # per-level durations: the same call with events around every level
+    m.set_level_timing(True)
+    for _ in range(min(args.steps, 5)):
+        step()
+    lvl = m.info()
+    m.set_level_timing(False)
+    levels = [{"level": k, "ms": round(v, 4), "work_items": it}
+              for k, (v, it) in enumerate(zip(lvl["level_ms"], lvl["items"]))]
+
     # accuracy: a seeded sample of problems (the largest 1D and 2D ones
     # included) against numpy's FP64 FFT convolution
     g = np.random.default_rng(7)
@@ -650,8 +659,8 @@ def run_c5(args, world, dist):
                         "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
                         "peak_source": "measured, MEASURED_PEAKS.json hbm_gbs"
                         if peak_kind == "measured" else "fallback 6650 GB/s",
-                        "kernel": f"pac_queue_kernel x{info['nlevels']} (one per level)",
-                        "algorithmic_bytes_per_step": alg_bytes},
+                        "kernel": f"pac_queue_kernel, {info['nlevels']} levels",
+                        "algorithmic_bytes_per_step": alg_bytes, "levels": levels},
            "gpu_launches": int(info["nlevels"] * args.steps), "clocks": clocks,
            "filter_spectrum_ms": round(spectrum_ms, 3),
            "rel_l2_vs_numpy_fp64": max(errs), "sampled_problems": len(errs)}

@@ -87,6 +87,7 @@ def _declare(L):
     L.pac_multi_filter_spectra.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp]
     L.pac_multi_convolve.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]
     L.pac_multi_get_info.argtypes = [_vp, C.POINTER(MultiInfo)]
+    L.pac_multi_set_level_timing.argtypes = [_vp, i]
     L.pac_status_string.restype = C.c_char_p
     L.pac_status_string.argtypes = [i]
     L.pac_last_error.restype = C.c_char_p
@@ -242,7 +243,8 @@ def dropin_twiddles(L, r, n):
 # ---------------------------------------------------------------------------
 class MultiInfo(C.Structure):
     _fields_ = [("nprob", C.c_int), ("nshapes", C.c_int), ("nlevels", C.c_int),
-                ("items", C.c_longlong * 8), ("elements", C.c_longlong), ("graph", C.c_int)]
+                ("items", C.c_longlong * 8), ("elements", C.c_longlong), ("graph", C.c_int),
+                ("level_ms", C.c_double * 8), ("timed_calls", C.c_longlong)]
 
 
 class MultiPlan:
@@ -276,7 +278,12 @@ class MultiPlan:
         check(self.L, self.L.pac_multi_get_info(self.h, C.byref(inf)), "pac_multi_get_info")
         return {"nprob": inf.nprob, "nshapes": inf.nshapes, "nlevels": inf.nlevels,
                 "items": list(inf.items[:inf.nlevels]), "elements": inf.elements,
-                "graph": inf.graph}
+                "graph": inf.graph, "level_ms": list(inf.level_ms[:inf.nlevels]),
+                "timed_calls": inf.timed_calls}
+
+    def set_level_timing(self, enable):
+        check(self.L, self.L.pac_multi_set_level_timing(self.h, 1 if enable else 0),
+              "pac_multi_set_level_timing")
 
     def close(self):
         if self.h:

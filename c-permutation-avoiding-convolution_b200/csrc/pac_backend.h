@@ -59,13 +59,13 @@ long long be_launch_count();
 
 // Persistent launch over a device work queue (pac_multi.cpp): the CTAs take
 // work items from *counter (zeroed beforehand) until `total` are done; item
-// i belongs to descriptor k with starts[k] <= i < starts[k + 1] and is CTA
-// i - starts[k] of that pass.  descs (ndesc) and starts (ndesc + 1) live in
+// i belongs to descriptor k = item_desc[i] and is CTA i - starts[k] of that
+// pass.  descs (ndesc), starts (ndesc + 1) and item_desc (total) live in
 // device memory; smem is the largest shared-memory size of the passes.
 int be_queue_prepare(int elem_bytes, int b2, size_t smem);  // outside graph capture
-int be_launch_queue(const PassDesc* descs, const long long* starts, int ndesc, long long total,
-                    unsigned long long* counter, int elem_bytes, int b2, size_t smem,
-                    void* stream);
+int be_launch_queue(const PassDesc* descs, const long long* starts, const int* item_desc,
+                    int ndesc, long long total, unsigned long long* counter, int elem_bytes,
+                    int b2, size_t smem, void* stream);
 // CUDA graphs: capture what a thread issues on `stream` between begin and
 // end, then replay it.  be_graph_supported() is 0 where nothing can be
 // captured (the host replay), and callers then issue the work directly.

@@ -91,13 +91,15 @@ __global__ void __launch_bounds__(NT, MINB) pac_special_kernel(const PassDesc d)
 
 // Persistent CTAs over a device work queue (many passes of different
 // geometry in one launch, pac_multi.cpp): thread 0 takes the next item from
-// the counter and finds its pass by binary search over the item starts; the
-// pass descriptor is copied into shared memory and the CTA runs that pass's
-// CTA `item - starts[k]` with the run-time geometry of pac_pass_kernel.
+// the counter and reads its pass k from the item table; the pass descriptor
+// is copied into shared memory (unless the CTA's previous item had the same
+// pass) and the CTA runs that pass's CTA `item - starts[k]` with the
+// run-time geometry of pac_pass_kernel.
 template <typename T, int B2>
 __global__ void __launch_bounds__(256) pac_queue_kernel(const PassDesc* __restrict__ descs,
                                                         const long long* __restrict__ starts,
-                                                        int ndesc, long long total,
+                                                        const int* __restrict__ item_desc,
+                                                        long long total,
                                                         unsigned long long* counter) {
   extern __shared__ __align__(16) unsigned char pac_smem[];
   __shared__ PassDesc sd;
@@ -105,28 +107,24 @@ __global__ void __launch_bounds__(256) pac_queue_kernel(const PassDesc* __restri
   __shared__ long long s_item;
   __shared__ int s_k;
   static_assert(sizeof(PassDesc) % sizeof(int) == 0, "descriptor copy in words");
+  int have = -1;  // pass whose descriptor sd holds
   for (;;) {
     if (threadIdx.x == 0) {
       const long long it = (long long)atomicAdd(counter, 1ULL);
-      int lo = 0, hi = ndesc - 1;
-      if (it < total) {
-        while (lo < hi) {  // largest k with starts[k] <= it
-          const int mid = (lo + hi + 1) >> 1;
-          if (starts[mid] <= it) lo = mid;
-          else hi = mid - 1;
-        }
-      }
       s_item = it;
-      s_k = lo;
+      s_k = it < total ? item_desc[it] : 0;
     }
     __syncthreads();
     const long long it = s_item;
     if (it >= total) break;
     const int k = s_k;
-    const int* src = reinterpret_cast<const int*>(descs + k);
-    int* dst = reinterpret_cast<int*>(&sd);
-    for (int i = threadIdx.x; i < (int)(sizeof(PassDesc) / sizeof(int)); i += blockDim.x)
-      dst[i] = src[i];
+    if (k != have) {
+      const int* src = reinterpret_cast<const int*>(descs + k);
+      int* dst = reinterpret_cast<int*>(&sd);
+      for (int i = threadIdx.x; i < (int)(sizeof(PassDesc) / sizeof(int)); i += blockDim.x)
+        dst[i] = src[i];
+      have = k;
+    }
     __syncthreads();
     const long long cta = it - starts[k];
     T* sre = reinterpret_cast<T*>(pac_smem);
@@ -744,9 +742,10 @@ int be_queue_prepare(int elem_bytes, int b2, size_t smem) {
   return queue_prepare(elem_bytes, b2, smem, nullptr);
 }
 
-int be_launch_queue(const PassDesc* descs, const long long* starts, int ndesc, long long total,
-                    unsigned long long* counter, int elem_bytes, int b2, size_t smem,
-                    void* stream) {
+int be_launch_queue(const PassDesc* descs, const long long* starts, const int* item_desc,
+                    int ndesc, long long total, unsigned long long* counter, int elem_bytes,
+                    int b2, size_t smem, void* stream) {
+  (void)ndesc;
   if (total <= 0) return PAC_SUCCESS;
   int per_sm = 0;
   PAC_TRY_BE(queue_prepare(elem_bytes, b2, smem, &per_sm));
@@ -754,7 +753,8 @@ int be_launch_queue(const PassDesc* descs, const long long* starts, int ndesc, l
   if (grid > total) grid = total;
   cudaStream_t s = (cudaStream_t)stream;
 #define PAC_Q(T, B)                                                                        \
-  pac_queue_kernel<T, B><<<(unsigned)grid, 256, smem, s>>>(descs, starts, ndesc, total, counter)
+  pac_queue_kernel<T, B><<<(unsigned)grid, 256, smem, s>>>(descs, starts, item_desc, total, \
+                                                             counter)
   if (elem_bytes == 8) {
     if (b2 == 1) PAC_Q(double, 1);
     else if (b2 == 2) PAC_Q(double, 2);

@@ -387,12 +387,11 @@ long long be_launch_count() { return g_launches.load(); }
 // work-queue launch: the items in queue order, one CTA each (the queue's
 // order is the one a single persistent CTA would take)
 template <typename T, int B2>
-static void replay_queue(const PassDesc* descs, const long long* starts, int ndesc,
+static void replay_queue(const PassDesc* descs, const long long* starts, const int* item_desc,
                          long long total) {
   std::vector<long long> lb(128);
   for (long long it = 0; it < total; ++it) {
-    int k = 0;
-    while (k + 1 < ndesc && starts[k + 1] <= it) ++k;
+    const int k = item_desc[it];
     const PassDesc& d = descs[k];
     const long long cta = it - starts[k];
     std::vector<T> sm((size_t)2 * d.W * d.pitch, std::numeric_limits<T>::quiet_NaN());
@@ -404,16 +403,17 @@ static void replay_queue(const PassDesc* descs, const long long* starts, int nde
 
 int be_queue_prepare(int, int, size_t) { return PAC_SUCCESS; }
 
-int be_launch_queue(const PassDesc* descs, const long long* starts, int ndesc, long long total,
-                    unsigned long long* counter, int elem_bytes, int b2, size_t, void*) {
+int be_launch_queue(const PassDesc* descs, const long long* starts, const int* item_desc, int,
+                    long long total, unsigned long long* counter, int elem_bytes, int b2, size_t,
+                    void*) {
   if (elem_bytes == 8) {
-    if (b2 == 1) replay_queue<double, 1>(descs, starts, ndesc, total);
-    else if (b2 == 2) replay_queue<double, 2>(descs, starts, ndesc, total);
-    else replay_queue<double, 3>(descs, starts, ndesc, total);
+    if (b2 == 1) replay_queue<double, 1>(descs, starts, item_desc, total);
+    else if (b2 == 2) replay_queue<double, 2>(descs, starts, item_desc, total);
+    else replay_queue<double, 3>(descs, starts, item_desc, total);
   } else {
-    if (b2 == 1) replay_queue<float, 1>(descs, starts, ndesc, total);
-    else if (b2 == 2) replay_queue<float, 2>(descs, starts, ndesc, total);
-    else replay_queue<float, 3>(descs, starts, ndesc, total);
+    if (b2 == 1) replay_queue<float, 1>(descs, starts, item_desc, total);
+    else if (b2 == 2) replay_queue<float, 2>(descs, starts, item_desc, total);
+    else replay_queue<float, 3>(descs, starts, item_desc, total);
   }
   if (total > 0) *counter += (unsigned long long)total;
   g_launches++;

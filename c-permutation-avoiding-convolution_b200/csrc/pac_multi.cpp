@@ -1,7 +1,14 @@
 // pac_multi.cpp -- many convolutions of uneven shapes per call (pac.h,
 // pac_multi_*): one plan per distinct shape, every problem's passes grouped
-// into levels, each level one persistent work-queue launch, the levels of a
-// buffer set captured once into a CUDA graph.
+// into levels (the k-th pass of every problem), each level run by
+// persistent work-queue launches, the launches of a buffer set captured once
+// into a CUDA graph.
+//
+// A work-queue launch reserves the largest shared-memory tile of its passes
+// for every CTA, so a level is split by tile size into groups: passes with
+// tiles up to kSmallSmem go to one launch (several CTAs per SM), larger ones
+// to another, and the two run side by side on two streams (two branches of
+// the graph).
 #include <stdlib.h>
 #include <string.h>
 
@@ -32,15 +39,20 @@ using namespace pac;
 
 namespace {
 
-enum { kMaxLevels = 8 };
+enum { kMaxLevels = 8, kGroups = 2 };
+const size_t kSmallSmem = 72 * 1024;
 
-struct Level {
+// one work-queue launch: passes of one level and one tile-size class
+struct Group {
   int ndesc = 0;
   long long total = 0;  // work items (CTAs)
   size_t smem = 0;
   size_t desc_off = 0;   // byte offsets into the device block
   size_t start_off = 0;
+  size_t item_off = 0;
 };
+
+size_t round256(size_t v) { return (v + 255) / 256 * 256; }
 
 }  // namespace
 
@@ -56,22 +68,31 @@ struct pac_multi_s {
   std::mutex mu;
   const void* key[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   bool built = false;
-  std::vector<Level> levels;
-  void* dev = nullptr;  // descriptors, starts and counters of all levels
+  std::vector<std::vector<Group>> levels;  // per level: its non-empty groups
+  void* dev = nullptr;  // descriptors, starts, item tables and counters
   size_t dev_bytes = 0;
   size_t counter_off = 0;
+  void* side = nullptr;  // second stream for the small-tile groups
   void* graph = nullptr;
   void* graph_stream = nullptr;
+  // level timing (pac_multi_set_level_timing)
+  int timing = 0;
+  std::vector<void*> ev;
+  double level_ms[kMaxLevels] = {};
+  long long timed_calls = 0;
   ~pac_multi_s() {
+    for (void* e : ev) be_event_destroy(e);
     if (graph) be_graph_destroy(graph);
+    if (side) be_stream_destroy(side);
     if (dev) be_free(dev);
     for (pac_plan_t p : plans) pac_plan_destroy(p);
   }
 };
 
-// Gather every problem's pass list for the buffer set, group the passes into
-// levels, order each level's passes by tile size (largest first: the queue
-// hands out the long CTAs early) and upload descriptors and item starts.
+// Gather every problem's pass list for the buffer set, group the passes by
+// level and tile size, order each group's passes by tile size (largest
+// first: the queue hands out the long CTAs early) and upload descriptors,
+// item starts and the item -> pass tables.
 static int build_levels(pac_multi_s* m, const void* x_re, const void* x_im, const void* h_re,
                         const void* h_im, void* y_re, void* y_im, void* stream) {
   struct Item {
@@ -80,8 +101,9 @@ static int build_levels(pac_multi_s* m, const void* x_re, const void* x_im, cons
     size_t smem;
     long long work;  // elements per CTA
   };
-  std::vector<std::vector<Item>> lv;
+  std::vector<std::vector<Item>> lv[kGroups];
   const size_t B = (size_t)m->bytes;
+  size_t nlev = 0;
   for (int p = 0; p < m->nprob; ++p) {
     const size_t o = (size_t)m->off[p] * B;
     std::vector<PassDesc> descs;
@@ -93,38 +115,57 @@ static int build_levels(pac_multi_s* m, const void* x_re, const void* x_im, cons
     if (descs.size() > (size_t)kMaxLevels)
       return set_error(PAC_ERROR_SIZE, "problem %d needs %zu passes (at most %d)", p,
                        descs.size(), (int)kMaxLevels);
-    if (lv.size() < descs.size()) lv.resize(descs.size());
-    for (size_t k = 0; k < descs.size(); ++k)
-      lv[k].push_back({descs[k], ctas[k], smem[k], (long long)descs[k].W << descs[k].logL});
-  }
-  m->levels.assign(lv.size(), Level());
-  size_t bytes = 0;
-  for (size_t k = 0; k < lv.size(); ++k) {
-    std::stable_sort(lv[k].begin(), lv[k].end(),
-                     [](const Item& a, const Item& b) { return a.work > b.work; });
-    Level& L = m->levels[k];
-    L.ndesc = (int)lv[k].size();
-    L.desc_off = bytes;
-    bytes += (sizeof(PassDesc) * L.ndesc + 255) / 256 * 256;
-    L.start_off = bytes;
-    bytes += (sizeof(long long) * (L.ndesc + 1) + 255) / 256 * 256;
-  }
-  m->counter_off = bytes;
-  bytes += 256;
-  std::vector<unsigned char> host(bytes, 0);
-  for (size_t k = 0; k < lv.size(); ++k) {
-    Level& L = m->levels[k];
-    PassDesc* d = (PassDesc*)(host.data() + L.desc_off);
-    long long* st = (long long*)(host.data() + L.start_off);
-    long long acc = 0;
-    for (int i = 0; i < L.ndesc; ++i) {
-      d[i] = lv[k][i].d;
-      st[i] = acc;
-      acc += lv[k][i].ctas;
-      L.smem = std::max(L.smem, lv[k][i].smem);
+    nlev = std::max(nlev, descs.size());
+    for (int g = 0; g < kGroups; ++g)
+      if (lv[g].size() < nlev) lv[g].resize(nlev);
+    for (size_t k = 0; k < descs.size(); ++k) {
+      const int g = smem[k] <= kSmallSmem ? 1 : 0;
+      lv[g][k].push_back({descs[k], ctas[k], smem[k], (long long)descs[k].W << descs[k].logL});
     }
-    st[L.ndesc] = acc;
-    L.total = acc;
+  }
+  m->levels.assign(nlev, {});
+  size_t bytes = 0;
+  for (size_t k = 0; k < nlev; ++k)
+    for (int g = 0; g < kGroups; ++g) {
+      auto& items = lv[g][k];
+      if (items.empty()) continue;
+      std::stable_sort(items.begin(), items.end(),
+                       [](const Item& a, const Item& b) { return a.work > b.work; });
+      Group G;
+      G.ndesc = (int)items.size();
+      for (auto& it : items) {
+        G.total += it.ctas;
+        G.smem = std::max(G.smem, it.smem);
+      }
+      G.desc_off = bytes;
+      bytes += round256(sizeof(PassDesc) * G.ndesc);
+      G.start_off = bytes;
+      bytes += round256(sizeof(long long) * (G.ndesc + 1));
+      G.item_off = bytes;
+      bytes += round256(sizeof(int) * (size_t)G.total);
+      m->levels[k].push_back(G);
+    }
+  m->counter_off = bytes;
+  bytes += round256(sizeof(unsigned long long) * kMaxLevels * kGroups);
+  std::vector<unsigned char> host(bytes, 0);
+  for (size_t k = 0; k < nlev; ++k) {
+    size_t gi = 0;
+    for (int g = 0; g < kGroups; ++g) {
+      const auto& items = lv[g][k];
+      if (items.empty()) continue;
+      const Group& G = m->levels[k][gi++];
+      PassDesc* d = (PassDesc*)(host.data() + G.desc_off);
+      long long* st = (long long*)(host.data() + G.start_off);
+      int* tab = (int*)(host.data() + G.item_off);
+      long long acc = 0;
+      for (int i = 0; i < G.ndesc; ++i) {
+        d[i] = items[i].d;
+        st[i] = acc;
+        for (long long c = 0; c < items[i].ctas; ++c) tab[acc + c] = i;
+        acc += items[i].ctas;
+      }
+      st[G.ndesc] = acc;
+    }
   }
   if (m->dev_bytes < bytes) {
     if (m->dev) PAC_TRY(be_free(m->dev));
@@ -136,21 +177,58 @@ static int build_levels(pac_multi_s* m, const void* x_re, const void* x_im, cons
   PAC_TRY(be_memcpy(m->dev, host.data(), bytes, CPY_H2D, stream));
   // the host staging vector dies here: wait for the copy
   PAC_TRY(be_stream_sync(stream));
-  for (auto& L : m->levels) PAC_TRY(be_queue_prepare(m->bytes, m->b2, L.smem));
+  for (auto& groups : m->levels)
+    for (auto& G : groups) PAC_TRY(be_queue_prepare(m->bytes, m->b2, G.smem));
+  if (!m->side) PAC_TRY(be_stream_create(&m->side));
   return PAC_SUCCESS;
 }
 
-// counters to zero, then one work-queue launch per level
-static int issue_levels(pac_multi_s* m, void* stream) {
+static int launch_group(pac_multi_s* m, const Group& G, unsigned long long* cnt, void* stream) {
   char* dev = (char*)m->dev;
-  unsigned long long* cnt = (unsigned long long*)(dev + m->counter_off);
-  PAC_TRY(be_memset(cnt, 0, sizeof(unsigned long long) * kMaxLevels, stream));
+  return be_launch_queue((const PassDesc*)(dev + G.desc_off),
+                         (const long long*)(dev + G.start_off), (const int*)(dev + G.item_off),
+                         G.ndesc, G.total, cnt, m->bytes, m->b2, G.smem, stream);
+}
+
+// counters to zero, then every level: its groups side by side (the second
+// group on the side stream, forked from and joined back into `stream`);
+// with `ev`, event k is recorded on `stream` before level k and the last
+// one after the last level
+static int issue_levels(pac_multi_s* m, void* stream, void** ev = nullptr) {
+  unsigned long long* cnt = (unsigned long long*)((char*)m->dev + m->counter_off);
+  PAC_TRY(be_memset(cnt, 0, sizeof(unsigned long long) * kMaxLevels * kGroups, stream));
   for (size_t k = 0; k < m->levels.size(); ++k) {
-    const Level& L = m->levels[k];
-    PAC_TRY(be_launch_queue((const PassDesc*)(dev + L.desc_off),
-                            (const long long*)(dev + L.start_off), L.ndesc, L.total, cnt + k,
-                            m->bytes, m->b2, L.smem, stream));
+    const auto& groups = m->levels[k];
+    unsigned long long* c = cnt + k * kGroups;
+    if (ev) PAC_TRY(be_event_record(ev[k], stream));
+    if (groups.size() == 1) {
+      PAC_TRY(launch_group(m, groups[0], c, stream));
+      continue;
+    }
+    PAC_TRY(be_stream_wait(m->side, stream));
+    PAC_TRY(launch_group(m, groups[0], c, stream));
+    PAC_TRY(launch_group(m, groups[1], c + 1, m->side));
+    PAC_TRY(be_stream_wait(stream, m->side));
   }
+  if (ev) PAC_TRY(be_event_record(ev[m->levels.size()], stream));
+  return PAC_SUCCESS;
+}
+
+// a timed call: levels issued directly with events around them
+static int issue_timed(pac_multi_s* m, void* stream) {
+  const size_t n = m->levels.size();
+  while (m->ev.size() < n + 1) {
+    void* e = nullptr;
+    PAC_TRY(be_event_create(&e));
+    m->ev.push_back(e);
+  }
+  PAC_TRY(issue_levels(m, stream, m->ev.data()));
+  for (size_t k = 0; k < n; ++k) {
+    float ms = 0.f;
+    PAC_TRY(be_event_elapsed(m->ev[k], m->ev[k + 1], &ms));
+    m->level_ms[k] += ms;
+  }
+  m->timed_calls++;
   return PAC_SUCCESS;
 }
 
@@ -249,6 +327,7 @@ PAC_API int pac_multi_convolve(pac_multi_t m, const void* x_re, const void* x_im
     memcpy(m->key, key, sizeof(key));
     m->built = true;
   }
+  if (m->timing) return issue_timed(m, stream);
   if (stream == nullptr || !be_graph_supported()) return issue_levels(m, stream);
   if (m->graph && m->graph_stream != stream) {
     be_graph_destroy(m->graph);
@@ -277,9 +356,23 @@ PAC_API int pac_multi_get_info(pac_multi_t m, pac_multi_info_t* info) {
   info->nshapes = (int)m->plans.size();
   info->nlevels = (int)m->levels.size();
   for (size_t k = 0; k < m->levels.size() && k < kMaxLevels; ++k)
-    info->items[k] = m->levels[k].total;
+    for (auto& G : m->levels[k]) info->items[k] += G.total;
   info->elements = m->off[m->nprob];
   info->graph = m->graph ? 1 : 0;
+  info->timed_calls = m->timed_calls;
+  for (size_t k = 0; k < m->levels.size() && k < kMaxLevels; ++k)
+    info->level_ms[k] = m->timed_calls ? m->level_ms[k] / (double)m->timed_calls : 0.0;
+  return PAC_SUCCESS;
+}
+
+PAC_API int pac_multi_set_level_timing(pac_multi_t m, int enable) {
+  if (!m) return set_error(PAC_ERROR_INVALID_VALUE, "pac_multi_set_level_timing: NULL");
+  std::lock_guard<std::mutex> g(m->mu);
+  m->timing = enable ? 1 : 0;
+  if (enable) {
+    for (auto& v : m->level_ms) v = 0.0;
+    m->timed_calls = 0;
+  }
   return PAC_SUCCESS;
 }
 

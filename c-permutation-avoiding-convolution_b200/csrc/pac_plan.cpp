@@ -127,8 +127,13 @@ static int build_schedule(Schedule& s, int rank, const int* logs, int b2, int by
     if (nf > PAC_MAX_FACTORS)
       return set_error(PAC_ERROR_SIZE, "axis %d needs %d factors (at most %d)", a, nf,
                        (int)PAC_MAX_FACTORS);
-    std::vector<int> parts(nf, digits / nf);
-    for (int i = 0; i < digits % nf; ++i) parts[nf - 1 - i]++;
+    // the innermost factor (contiguous lines, the fused pass of a
+    // convolution) as long as one CTA holds; the outer factors (column
+    // passes, whose tiles grow with the column length) share the rest evenly
+    std::vector<int> parts(nf, 0);
+    parts[nf - 1] = nf == 1 ? digits : dmax;
+    const int rest = digits - parts[nf - 1];
+    for (int f = 0; f < nf - 1; ++f) parts[f] = rest / (nf - 1) + (f < rest % (nf - 1) ? 1 : 0);
     for (int f = 0; f < nf; ++f) s.vax.push_back({parts[f] * b2, a, f == 0, f == nf - 1});
   }
   for (auto& v : s.vax) s.rad.push_back(radix_schedule(v.log, b2));

@@ -165,13 +165,15 @@ PAC_API int pac_convolve_1d_noalloc(const double* x_re, const double* x_im, cons
  * plan and twiddles.
  *
  * pac_multi_convolve runs every problem's convolution passes level by level
- * (level k = the k-th pass of every problem that has one): each level is
- * ONE persistent launch whose CTAs take work items (pass, tile) from a
- * device work queue, largest tiles first, so small and large problems share
- * the GPU.  With a non-NULL stream the levels are captured once into a CUDA
- * graph per set of buffer addresses and replayed afterwards (the first call
- * for new addresses captures; later calls launch the graph).  Calls on one
- * multi-plan are serialised by a lock. */
+ * (level k = the k-th pass of every problem that has one): a level is one
+ * persistent launch whose CTAs take work items (pass, tile) from a device
+ * work queue, largest tiles first, so small and large problems share the
+ * GPU -- or two such launches side by side when the level mixes tiles of
+ * more and less than 72 KB of shared memory.  With a non-NULL stream the
+ * launches are captured once into a CUDA graph per set of buffer addresses
+ * and replayed afterwards (the first call for new addresses captures; later
+ * calls launch the graph).  Calls on one multi-plan are serialised by a
+ * lock. */
 typedef struct pac_multi_s* pac_multi_t;
 
 /* ranks[p] in 1..3; dims holds 3 entries per problem (the first ranks[p]
@@ -194,12 +196,19 @@ PAC_API int pac_multi_convolve(pac_multi_t multi, const void* x_re, const void* 
 typedef struct {
   int nprob;
   int nshapes;            /* distinct shapes (plans) */
-  int nlevels;            /* launches per pac_multi_convolve */
+  int nlevels;            /* levels of passes per pac_multi_convolve */
   long long items[8];     /* work items (CTAs) of each level */
   long long elements;     /* total elements of one packed array */
   int graph;              /* 1 once a CUDA graph replays the levels */
+  double level_ms[8];     /* per-level mean time of the timed calls */
+  long long timed_calls;  /* calls behind level_ms */
 } pac_multi_info_t;
 PAC_API int pac_multi_get_info(pac_multi_t multi, pac_multi_info_t* info);
+/* Level timing: while enabled, pac_multi_convolve issues the levels
+ * directly (no graph), records a CUDA event around every level on the
+ * caller's stream and waits for them (calls become synchronous);
+ * pac_multi_get_info reports the per-level means.  Enabling resets them. */
+PAC_API int pac_multi_set_level_timing(pac_multi_t multi, int enable);
 
 /* y = scale * x .* h elementwise over n complex FP64 values (the product
  * loop of convolution.c:55-62 on its own; the reference's convolution
