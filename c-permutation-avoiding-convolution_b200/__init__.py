@@ -60,6 +60,8 @@ class PacError(RuntimeError):
 def _declare(L):
     i, ll, d, sz = C.c_int, C.c_longlong, C.c_double, C.c_size_t
     L.pac_plan_create.argtypes = [C.POINTER(_vp), i, C.POINTER(i), i, i, i]
+    L.pac_plan_create_axes.argtypes = [C.POINTER(_vp), i, C.POINTER(i), C.POINTER(i), i, i]
+    L.pac_plan_get_info.argtypes = [_vp, C.POINTER(PlanInfo)]
     L.pac_plan_destroy.argtypes = [_vp]
     L.pac_filter_spectrum.argtypes = [_vp, _vp, _vp, i, _vp, _vp, d, _vp]
     L.pac_convolve.argtypes = [_vp, _vp, _vp, _vp, _vp, i, _vp, _vp, d, _vp]
@@ -241,6 +243,15 @@ def dropin_twiddles(L, r, n):
 # ---------------------------------------------------------------------------
 # native plan API (device pointers)
 # ---------------------------------------------------------------------------
+class PlanInfo(C.Structure):
+    """pac_plan_info_t"""
+    _fields_ = [("n_elements", C.c_longlong), ("batch", C.c_longlong), ("rank", C.c_int),
+                ("dims", C.c_int * 3), ("digit_base", C.c_int), ("form", C.c_int),
+                ("element_bytes", C.c_int), ("conv_passes", C.c_int),
+                ("transform_passes", C.c_int), ("workspace_bytes", C.c_size_t),
+                ("digit_bases", C.c_int * 3)]
+
+
 class MultiInfo(C.Structure):
     _fields_ = [("nprob", C.c_int), ("nshapes", C.c_int), ("nlevels", C.c_int),
                 ("items", C.c_longlong * 8), ("elements", C.c_longlong), ("graph", C.c_int),
@@ -304,8 +315,13 @@ class Plan:
         self.L = L
         self.h = _vp()
         arr = (C.c_int * len(dims))(*dims)
-        check(L, L.pac_plan_create(C.byref(self.h), len(dims), arr, batch, digit_base, form),
-              "pac_plan_create")
+        if isinstance(digit_base, (tuple, list)):  # one digit base per axis
+            bases = (C.c_int * len(dims))(*digit_base)
+            check(L, L.pac_plan_create_axes(C.byref(self.h), len(dims), arr, bases, batch, form),
+                  "pac_plan_create_axes")
+        else:
+            check(L, L.pac_plan_create(C.byref(self.h), len(dims), arr, batch, digit_base, form),
+                  "pac_plan_create")
         self.dims = tuple(dims)
         self.batch = batch
         self.form = form

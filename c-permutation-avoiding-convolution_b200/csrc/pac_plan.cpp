@@ -66,6 +66,7 @@ struct VAx {
   int axis;     // real axis index
   int first;    // first factor of its axis
   int last;     // last (innermost) factor of its axis
+  int b2;       // log2 of its axis's digit base
 };
 
 struct Schedule {
@@ -114,13 +115,14 @@ static int max_factor_log(int bytes, int b2) {
   return lmax - lmax % b2;
 }
 
-static int build_schedule(Schedule& s, int rank, const int* logs, int b2, int bytes) {
+static int build_schedule(Schedule& s, int rank, const int* logs, const int* b2s, int bytes) {
   s.bytes = bytes;
-  s.b2 = b2;
-  int lmax = max_factor_log(bytes, b2);
+  s.b2 = b2s[rank - 1];
   for (int a = 0; a < rank; ++a) {
     int lg = logs[a];
     if (lg == 0) continue;
+    const int b2 = b2s[a];
+    const int lmax = max_factor_log(bytes, b2);
     int digits = lg / b2;
     int dmax = lmax / b2;
     int nf = (digits + dmax - 1) / dmax;
@@ -134,9 +136,9 @@ static int build_schedule(Schedule& s, int rank, const int* logs, int b2, int by
     parts[nf - 1] = nf == 1 ? digits : dmax;
     const int rest = digits - parts[nf - 1];
     for (int f = 0; f < nf - 1; ++f) parts[f] = rest / (nf - 1) + (f < rest % (nf - 1) ? 1 : 0);
-    for (int f = 0; f < nf; ++f) s.vax.push_back({parts[f] * b2, a, f == 0, f == nf - 1});
+    for (int f = 0; f < nf; ++f) s.vax.push_back({parts[f] * b2, a, f == 0, f == nf - 1, b2});
   }
-  for (auto& v : s.vax) s.rad.push_back(radix_schedule(v.log, b2));
+  for (auto& v : s.vax) s.rad.push_back(radix_schedule(v.log, v.b2));
   // stage twiddle tables
   std::vector<std::pair<int, int>> specs;
   long long total = 0;
@@ -189,7 +191,8 @@ struct pac_plan_s {
   int dims[3] = {1, 1, 1};
   int logs[3] = {0, 0, 0};
   long long batch = 1;
-  int b2 = 1;
+  int b2 = 1;                // axis 0's digit base (log2)
+  int b2s[3] = {1, 1, 1};    // every axis's
   int form = PAC_FORM_F64;
   long long N = 1;
   pac::Schedule main;                     // storage type of the form
@@ -220,6 +223,7 @@ struct PassSpec {
   int threads;
   size_t smem;
   bool oop;  // cannot run in place
+  int b2;    // log2 digit base of the pass's axis
 };
 
 // geometry of a pass over factor vi for `batch` problems
@@ -290,6 +294,7 @@ static PassSpec make_pass(const Schedule& s, int vi, long long batch, long long 
   p.threads = threads;
   p.smem = (size_t)2 * d.W * d.pitch * esz;
   p.oop = false;
+  p.b2 = v.b2;
   return p;
 }
 
@@ -305,7 +310,7 @@ static void apply_special(const Schedule& s, PassSpec& p) {
   const char* cvar = getenv("PAC_CLUSTER_VARIANT");
   if (d.logS > 0 && cvar != nullptr) {
     int logC = 0;
-    if (cluster_geometry(s.bytes, s.b2, d.mode, d.sign, d.logL, &logW, &logC, &nt, atoi(cvar)) &&
+    if (cluster_geometry(s.bytes, p.b2, d.mode, d.sign, d.logL, &logW, &logC, &nt, atoi(cvar)) &&
         logW <= d.logS && (d.nlines & ((1LL << logW) - 1)) == 0) {
       d.W = 1 << logW;
       d.logW = logW;
@@ -324,7 +329,7 @@ static void apply_special(const Schedule& s, PassSpec& p) {
   // for the tensor maps)
   const char* pipe = getenv("PAC_PIPE");
   if (d.logS > 0 && cvar == nullptr && pipe != nullptr && atoi(pipe) != 0 &&
-      pipe_geometry(s.bytes, s.b2, d.mode, d.sign, d.logL, &logW, &nt) && logW <= d.logS &&
+      pipe_geometry(s.bytes, p.b2, d.mode, d.sign, d.logL, &logW, &nt) && logW <= d.logS &&
       (d.nlines & ((1LL << logW) - 1)) == 0 && (d.nlines >> d.logS) < (1LL << 31) &&
       ((uintptr_t)d.in_re | (uintptr_t)d.in_im) % 16 == 0) {
     d.W = 1 << logW;
@@ -342,9 +347,9 @@ static void apply_special(const Schedule& s, PassSpec& p) {
   }
   const char* var = getenv("PAC_SPECIAL_VARIANT");
   const int variant = var ? atoi(var) : 0;
-  if (!special_geometry(s.bytes, s.b2, d.mode, d.sign, d.logL, d.logS > 0 ? 1 : 0, &logW, &nt,
+  if (!special_geometry(s.bytes, p.b2, d.mode, d.sign, d.logL, d.logS > 0 ? 1 : 0, &logW, &nt,
                         variant) &&
-      !special_geometry(s.bytes, s.b2, d.mode, d.sign, d.logL, d.logS > 0 ? 1 : 0, &logW, &nt))
+      !special_geometry(s.bytes, p.b2, d.mode, d.sign, d.logL, d.logS > 0 ? 1 : 0, &logW, &nt))
     return;
   const long long W = 1LL << logW;
   if ((d.nlines & (W - 1)) != 0) return;
@@ -360,7 +365,7 @@ static void apply_special(const Schedule& s, PassSpec& p) {
 }
 
 static int launch(const Schedule& s, PassSpec& p, void* stream) {
-  return be_launch_pass(p.d, s.bytes, s.b2, p.grid, p.threads, p.smem, stream);
+  return be_launch_pass(p.d, s.bytes, p.b2, p.grid, p.threads, p.smem, stream);
 }
 
 // Launch a pass list; with pass timing enabled, bracket every pass with
@@ -620,7 +625,7 @@ static int build_schedule_in_arena(Schedule& s, int logn, Arena& ar, void* strea
     if (nf > PAC_MAX_FACTORS) return set_error(PAC_ERROR_SIZE, "too many factors");
     std::vector<int> parts(nf, logn / nf);
     for (int i = 0; i < logn % nf; ++i) parts[nf - 1 - i]++;
-    for (int f = 0; f < nf; ++f) s.vax.push_back({parts[f], 0, f == 0, f == nf - 1});
+    for (int f = 0; f < nf; ++f) s.vax.push_back({parts[f], 0, f == 0, f == nf - 1, 1});
   }
   for (auto& v : s.vax) s.rad.push_back(radix_schedule(v.log, 1));
   long long total = 0;
@@ -708,15 +713,18 @@ static int ilog2_exact(long long v, int b2) {
 
 extern "C" {
 
-PAC_API int pac_plan_create(pac_plan_t* plan, int rank, const int* dims, int batch,
-                            int digit_base, int form) {
-  if (!plan || !dims || rank < 1 || rank > 3 || batch < 1)
+PAC_API int pac_plan_create_axes(pac_plan_t* plan, int rank, const int* dims,
+                                 const int* digit_bases, int batch, int form) {
+  if (!plan || !dims || !digit_bases || rank < 1 || rank > 3 || batch < 1)
     return set_error(PAC_ERROR_INVALID_VALUE, "pac_plan_create: invalid rank/dims/batch");
-  if (digit_base == 0) digit_base = 2;
-  int b2 = digit_base == 2 ? 1 : digit_base == 4 ? 2 : digit_base == 8 ? 3 : 0;
-  if (!b2)
-    return set_error(PAC_ERROR_UNSUPPORTED_RADIX, "pac_plan_create: digit base %d not in {2,4,8}",
-                     digit_base);
+  int b2s[3] = {1, 1, 1};
+  for (int a = 0; a < rank; ++a) {
+    const int base = digit_bases[a] == 0 ? 2 : digit_bases[a];
+    b2s[a] = base == 2 ? 1 : base == 4 ? 2 : base == 8 ? 3 : 0;
+    if (!b2s[a])
+      return set_error(PAC_ERROR_UNSUPPORTED_RADIX,
+                       "pac_plan_create: digit base %d (axis %d) not in {2,4,8}", base, a);
+  }
   if (form != PAC_FORM_F64 && form != PAC_FORM_F32)
     return set_error(PAC_ERROR_INVALID_VALUE, "pac_plan_create: unknown form %d", form);
   int st = be_init();
@@ -724,31 +732,38 @@ PAC_API int pac_plan_create(pac_plan_t* plan, int rank, const int* dims, int bat
   std::unique_ptr<pac_plan_s> p(new pac_plan_s());
   p->rank = rank;
   p->batch = batch;
-  p->b2 = b2;
+  p->b2 = b2s[0];
   p->form = form;
   long long N = 1;
   for (int a = 0; a < rank; ++a) {
-    int lg = ilog2_exact(dims[a], b2);
+    int lg = ilog2_exact(dims[a], b2s[a]);
     if (lg < 0)
       return set_error(PAC_ERROR_NOT_POWER, "pac_plan_create: axis %d length %d is not a power of %d",
-                       a, dims[a], digit_base);
+                       a, dims[a], 1 << b2s[a]);
     p->dims[a] = dims[a];
     p->logs[a] = lg;
+    p->b2s[a] = b2s[a];
     N *= dims[a];
   }
   if (N * (long long)batch > (1LL << 40) || N > (1LL << 31))
     return set_error(PAC_ERROR_SIZE, "pac_plan_create: problem too large");
   p->N = N;
   int bytes = form == PAC_FORM_F64 ? 8 : 4;
-  st = build_schedule(p->main, rank, p->logs, b2, bytes);
+  st = build_schedule(p->main, rank, p->logs, b2s, bytes);
   if (st != PAC_SUCCESS) return st;
   if (bytes != 8) {
     p->s64.reset(new Schedule());
-    st = build_schedule(*p->s64, rank, p->logs, b2, 8);
+    st = build_schedule(*p->s64, rank, p->logs, b2s, 8);
     if (st != PAC_SUCCESS) return st;
   }
   *plan = p.release();
   return PAC_SUCCESS;
+}
+
+PAC_API int pac_plan_create(pac_plan_t* plan, int rank, const int* dims, int batch,
+                            int digit_base, int form) {
+  const int bases[3] = {digit_base, digit_base, digit_base};
+  return pac_plan_create_axes(plan, rank, dims, bases, batch, form);
 }
 
 PAC_API int pac_plan_destroy(pac_plan_t plan) {
@@ -764,6 +779,7 @@ PAC_API int pac_plan_get_info(pac_plan_t plan, pac_plan_info_t* info) {
   info->rank = plan->rank;
   for (int a = 0; a < 3; ++a) info->dims[a] = plan->dims[a];
   info->digit_base = 1 << plan->b2;
+  for (int a = 0; a < 3; ++a) info->digit_bases[a] = a < plan->rank ? 1 << plan->b2s[a] : 0;
   info->form = plan->form;
   info->element_bytes = plan->main.bytes;
   int m = (int)plan->main.vax.size();

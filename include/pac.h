@@ -84,6 +84,7 @@ typedef struct {
   int conv_passes;        /* kernel launches of one pac_convolve          */
   int transform_passes;   /* kernel launches of one forward transform     */
   size_t workspace_bytes; /* device workspace held by the plan            */
+  int digit_bases[3];     /* per axis (digit_base is axis 0's)            */
 } pac_plan_info_t;
 
 /* Plan for `batch` problems of shape dims[0..rank-1] (rank 1..3).  Every
@@ -93,6 +94,14 @@ typedef struct {
  * the tables are generated on the device in FP64. */
 PAC_API int pac_plan_create(pac_plan_t* plan, int rank, const int* dims, int batch,
                             int digit_base, int form);
+/* As pac_plan_create with one digit base per axis (digit_bases[a] in
+ * {2, 4, 8}, 0 picks 2): axis a's spectrum is in base-digit_bases[a] digit-
+ * reversed order, A^T = (P_b0 F) x (P_b1 F) x ...  No counterpart in the
+ * reference, which uses one radix for every axis (convolution_2d.c:41-47,
+ * convolution_3d.c:44-49) and so runs 512 x 256 x 128 at radix 2 only; here
+ * it runs at bases 8, 4 and 2. */
+PAC_API int pac_plan_create_axes(pac_plan_t* plan, int rank, const int* dims,
+                                 const int* digit_bases, int batch, int form);
 /* free_twiddles (twiddle_factors.c:133) */
 PAC_API int pac_plan_destroy(pac_plan_t plan);
 PAC_API int pac_plan_get_info(pac_plan_t plan, pac_plan_info_t* info);

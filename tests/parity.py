@@ -265,3 +265,48 @@ def check_multi(L, shapes, form, stream=False, seed=3):
             bad[(p, s)] = e
     assert not bad, bad
     return info
+
+
+def digit_reversal(base, n):
+    """index -> its base-`base` digit reversal (n a power of base)"""
+    k = int(round(np.log(n) / np.log(base)))
+    idx = np.arange(n)
+    out = np.zeros(n, dtype=np.int64)
+    v = idx.copy()
+    for _ in range(k):
+        out = out * base + v % base
+        v //= base
+    return out
+
+
+def check_axis_bases(L, dims, bases, form, batch=2):
+    """Plans with one digit base per axis: the convolution and the natural-
+    order FFT against numpy; A^T = P F, A = F P and conj(A) = n F^-1 P with
+    P the per-axis digit reversal (every axis in its own base)."""
+    g = rng(13)
+    shape = (batch,) + tuple(dims)
+    x = g.standard_normal(shape) + 1j * g.standard_normal(shape)
+    h = g.standard_normal(dims) + 1j * g.standard_normal(dims)
+    tol = TOL if form == pac.PAC_FORM_F64 else TOL_F32
+    axes = tuple(range(1, len(shape)))
+    y = native_conv(L, dims, batch, tuple(bases), form, x, h)
+    assert crel(y, fftconv(x, h[None], axes)) < tol
+    rev = np.ix_(*[digit_reversal(b, n) for b, n in zip(bases, dims)])
+    n = int(np.prod(dims))
+    for op in (pac.OP_AT, pac.OP_A, pac.OP_CONJ_A, pac.OP_FFT):
+        t = native_transform(L, dims, batch, tuple(bases), pac.PAC_FORM_F64, op, x)
+        for b in range(batch):
+            if op == pac.OP_AT:
+                want = np.fft.fftn(x[b])[rev]
+            elif op == pac.OP_A:
+                want = np.fft.fftn(x[b][rev])
+            elif op == pac.OP_CONJ_A:
+                want = n * np.fft.ifftn(x[b][rev])
+            else:
+                want = np.fft.fftn(x[b])
+            assert crel(t[b], want) < TOL, (op, b)
+    plan = pac.Plan(L, dims, 1, tuple(bases), form)
+    info = pac.PlanInfo()
+    pac.check(L, L.pac_plan_get_info(plan.h, C.byref(info)), "info")
+    plan.close()
+    assert list(info.digit_bases[:len(dims)]) == list(bases)

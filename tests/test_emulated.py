@@ -178,3 +178,11 @@ def test_multi_uneven_batch(emu, form):
     assert info["nprob"] == len(shapes) and info["nshapes"] == len(set(shapes))
     # the 3D shape has three factors: 5 passes, the deepest level count
     assert info["nlevels"] == 5 and info["graph"] == 0
+
+
+@pytest.mark.parametrize("dims,bases,form", [((64, 16, 8), (8, 4, 2), 0), ((64, 16, 8), (8, 4, 2), 1),
+                                              ((512, 64), (8, 4), 0), ((32, 8), (2, 8), 1),
+                                              ((4096, 16), (4, 2), 0)])
+def test_axis_bases(emu, dims, bases, form):
+    """One digit base per axis (pac_plan_create_axes)."""
+    P.check_axis_bases(emu, dims, bases, form)

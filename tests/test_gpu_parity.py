@@ -234,3 +234,12 @@ def test_multi_uneven_batch(lib, form, stream):
     shapes = W5 + [(2 ** 20,), (2048, 512), (16, 16, 16), (2,), (128, 4, 64)]
     info = P.check_multi(lib, shapes, form, stream=stream)
     assert info["graph"] == (1 if stream else 0)
+
+
+@pytest.mark.parametrize("dims,bases,form", [((64, 16, 8), (8, 4, 2), 0), ((512, 64), (8, 4), 1),
+                                              ((2 ** 15, 16), (8, 2), 0),
+                                              ((512, 256, 128), (8, 4, 2), 1)])
+def test_axis_bases(lib, dims, bases, form):
+    """One digit base per axis: 512 x 256 x 128 at bases 8, 4, 2 (the
+    reference runs it at radix 2 only)."""
+    P.check_axis_bases(lib, dims, bases, form, batch=1 if np.prod(dims) > 2 ** 20 else 2)
