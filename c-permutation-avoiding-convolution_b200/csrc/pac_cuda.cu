@@ -77,7 +77,7 @@ __global__ void __launch_bounds__(256) pac_pass_kernel(const PassDesc d) {
 template <typename T, int B2, int MODE, int SIGN, int LOGL, int COLS, int LOGW, int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB) pac_special_kernel(const PassDesc d) {
   constexpr int W = 1 << LOGW;
-  constexpr int PITCH = pitch_for((int)sizeof(T), LOGL, W);
+  constexpr int PITCH = pitch_for((int)sizeof(T), LOGL, W, COLS);
   using SP = Shape<LOGL, LOGW, PITCH, COLS>;
   extern __shared__ __align__(16) unsigned char pac_smem[];
   __shared__ long long s_lb[W];

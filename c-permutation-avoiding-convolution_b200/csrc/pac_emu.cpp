@@ -84,7 +84,7 @@ static void replay(const PassDesc& d, long long grid) {
 template <typename T, int B2, int MODE, int SIGN, int LOGL, int COLS, int LOGW, int NT>
 static void replay_special(const PassDesc& d, long long grid) {
   constexpr int W = 1 << LOGW;
-  constexpr int PITCH = pitch_for((int)sizeof(T), LOGL, W);
+  constexpr int PITCH = pitch_for((int)sizeof(T), LOGL, W, COLS);
   using SP = Shape<LOGL, LOGW, PITCH, COLS>;
   std::vector<T> sm((size_t)2 * W * PITCH);
   std::vector<long long> lb(W);

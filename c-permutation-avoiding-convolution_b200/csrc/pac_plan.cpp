@@ -356,7 +356,7 @@ static void apply_special(const Schedule& s, PassSpec& p) {
   if (d.logS > 0 && logW > d.logS) return;
   d.W = (int)W;
   d.logW = logW;
-  d.pitch = pitch_for(s.bytes, d.logL, d.W);
+  d.pitch = pitch_for(s.bytes, d.logL, d.W, d.logS > 0 ? 1 : 0);
   d.nthreads = nt;
   d.spec = 1;
   p.threads = nt;

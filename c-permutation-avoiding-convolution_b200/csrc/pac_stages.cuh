@@ -19,6 +19,15 @@ namespace pac {
 
 enum { IO_SMEM = 0, IO_GLOBAL = 1 };
 
+// FP32 column tiles of 8 lines pad every line by one element per 8 plus 8
+// per 128 (sidx_col32): their three stage patterns -- 8 lines x 4
+// consecutive rows (the stage next to global memory), 4 blocks of 128 x 8
+// butterflies of one line (the middle stage), 8 lines x 4 blocks of 8 (the
+// innermost stage) -- then fall on 32 distinct banks, which one pad element
+// per 32 leaves 2-way conflicted.
+PAC_HDC bool col_pad32(int bytes, int cols, int W) { return bytes == 4 && cols == 1 && W == 8; }
+PAC_HD int sidx_col32(int e) { return e + (e >> 3) + 8 * (e >> 7); }
+
 // geometry policy; -1 = read from the PassDesc at run time
 template <int LOGL_ = -1, int LOGW_ = -1, int PITCH_ = -1, int COLS_ = -1>
 struct Shape {
@@ -52,7 +61,10 @@ struct Shape {
   // shared-memory index of element e of line w: padded lines
   template <typename T>
   static PAC_HD int sm(const PassDesc& d, int w, int e) {
-    return w * pitch(d) + sidx<T>(e);
+    if constexpr (col_pad32((int)sizeof(T), COLS_, LOGW_ >= 0 ? 1 << LOGW_ : 0))
+      return w * pitch(d) + sidx_col32(e);
+    else
+      return w * pitch(d) + sidx<T>(e);
   }
 };
 using RtShape = Shape<>;
@@ -693,12 +705,13 @@ struct RadsImpl<LG, B2, std::integer_sequence<int, I...>> {
 template <int LG, int B2>
 using RadsFor = typename RadsImpl<LG, B2, std::make_integer_sequence<int, sched_n(LG, B2)>>::type;
 
-// shared-memory line pitch: one pad element every 16 (FP64) / 32 (FP32),
-// then skewed so that the W lines of a column tile start in different banks
-PAC_HDC int pitch_for(int bytes, int logL, int W) {
+// shared-memory line pitch: one pad element every 16 (FP64) / 32 (FP32)
+// (FP32 8-line column tiles: sidx_col32), then skewed so that the W lines
+// of a column tile start in different banks
+PAC_HDC int pitch_for(int bytes, int logL, int W, int cols = 0) {
   const int L = 1 << logL;
   const int SH = bytes == 8 ? 4 : 5, NB = bytes == 8 ? 16 : 32;
-  int pitch = L + (L >> SH);
+  int pitch = col_pad32(bytes, cols, W) ? L + (L >> 3) + 8 * (L >> 7) : L + (L >> SH);
   if (W > 1) {
     int want = (NB / (W < NB ? W : NB)) % NB;
     pitch += ((want - pitch % NB) % NB + NB) % NB;
