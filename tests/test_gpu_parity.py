@@ -122,6 +122,11 @@ def test_c4_3d_f64_against_oracle(lib, orc):
     ((256,), 3, 4, 1, True), ((4096,), 7, 4, 0, False),
     ((2048, 64), 1, 2, 0, False), ((64, 2048), 2, 2, 0, False), ((2048, 32), 1, 2, 1, False),
     ((32, 2048), 2, 2, 1, True),
+    # specialised geometries: 256-point rows and columns (FP32 16 lines, FP64 8),
+    # 512-point columns and 128-point rows, base-4 4096-point rows and
+    # 16-point columns
+    ((256, 16, 256), 1, 2, 1, False), ((256, 8, 256), 1, 2, 0, False),
+    ((512, 2, 128), 1, 2, 1, False), ((2 ** 16,), 2, 4, 0, False), ((2 ** 16,), 2, 4, 1, False),
     ((2 ** 20,), 2, 2, 0, False), ((2 ** 20,), 2, 2, 1, False)])
 def test_native_conv(lib, dims, batch, base, form, per):
     g = rng(21)
