@@ -159,6 +159,20 @@ PAC_HD void stage_bf(const PassDesc& d, long long cta, T* sre, T* sim, int logK_
   const int logell = logK - LR;
   int w, blk, j;
   bf_coords<SP>(d, logK, LR, src == IO_GLOBAL || dst == IO_GLOBAL, u, &w, &blk, &j);
+  if constexpr (sizeof(T) == 4 && SP::kCols == 0 && CLOGK >= 0) {
+    // FP32 rows, shared-memory stages of stride 8: a warp takes 8 blocks x 4
+    // butterflies instead of 4 x 8, so that its addresses 128 blk + j + 8 m
+    // (pad one per 32) fall on the distinct banks j + 4 blk
+    if constexpr (CLOGK - LR == 3 && SP::kLogL - CLOGK >= 3) {
+      if (src != IO_GLOBAL && dst != IO_GLOBAL) {
+        const int lbf = SP::kLogL - LR;
+        const int v = u & ((1 << lbf) - 1), hi = v >> 5;
+        w = u >> lbf;
+        j = (v & 3) + 4 * (hi & 1);
+        blk = ((v >> 2) & 7) + 8 * (hi >> 1);
+      }
+    }
+  }
   const int ell = 1 << logell;
   const int e0 = (blk << logK) + j;
   const T* ire = (const T*)d.in_re;
