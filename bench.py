@@ -2,7 +2,7 @@
 """Benchmark of the permutation-avoiding FFT convolution on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--config c3|c1|c2|c4|c4a|c5] [--form f64|f32]
+                    [--config c3|c1|c2|c4|c4a|c5] [--form f64|f32|tc]
 
 A step is one convolution of one batch of the configuration's synthetic
 input.  The default workload is C3: a 2D 2048 x 2048 complex FP64 circular
@@ -67,6 +67,7 @@ CONFIGS = {
 # the capture, its command line and the per-kernel figures are in
 # profiles/c3_2048x2048_passes.md.  ncu flushes L2 between kernels, so these
 # are cold-cache figures: reads equal the algorithmic reads of every pass.
+FORMS = {"f64": pac.PAC_FORM_F64, "f32": pac.PAC_FORM_F32, "tc": pac.PAC_FORM_TC}
 MEASURED_TRAFFIC = {("c3", "f64"): 337652480, ("c3", "f32"): 137580544}
 
 
@@ -258,7 +259,7 @@ def run_ours(args, world, dist):
     cfg = CONFIGS[args.config]
     dims, batch = cfg["dims"], cfg["batch"]
     N = int(np.prod(dims))
-    form = pac.PAC_FORM_F64 if args.form == "f64" else pac.PAC_FORM_F32
+    form = FORMS[args.form]
     tdt = torch.float64 if form == pac.PAC_FORM_F64 else torch.float32
     esz = 8 if form == pac.PAC_FORM_F64 else 4
     L = pac.load()
@@ -349,13 +350,14 @@ def run_ours(args, world, dist):
     step(0)
     torch.cuda.synchronize()
     rows = [0] if batch == 1 else [0, batch - 1]
-    errs = []
+    errs, maxs = [], []
     axes = tuple(range(len(dims)))
     Hf = np.fft.fftn(h)
     for b in rows:
         got = y[0][b].double().cpu().numpy() + 1j * y[1][b].double().cpu().numpy()
         want = np.fft.ifftn(np.fft.fftn(x[b], axes=axes) * Hf, axes=axes)
         errs.append(float(np.linalg.norm((got - want).ravel()) / np.linalg.norm(want.ravel())))
+        maxs.append(float(np.max(np.abs(got - want)) / np.max(np.abs(want))))
 
     peak, peak_kind = read_peaks()
     alg_bytes = 3 * batch * N * 2 * esz  # read x + read Hhat + write y
@@ -384,7 +386,8 @@ def run_ours(args, world, dist):
                             f"{per / 2**20:.0f} MiB; Hhat {N * esz * 2 / 2**20:.0f} MiB",
                       "parallelism": f"replicas x{world}"},
            "roofline": roofline, "gpu_launches": int(launches), "clocks": clocks,
-           "filter_spectrum_ms": round(spectrum_ms, 4), "rel_l2_vs_numpy_fp64": max(errs)}
+           "filter_spectrum_ms": round(spectrum_ms, 4), "rel_l2_vs_numpy_fp64": max(errs),
+           "max_err_vs_numpy_fp64": max(maxs)}
     out["config"]["l2_persisting_output"] = bool(l2_bytes)
     if l2_bytes:
         pac.check(L, L.pac_stream_set_l2_persisting(sp, None, 0), "l2")
@@ -399,7 +402,7 @@ def run_profile(args):
 
     cfg = CONFIGS[args.config]
     dims, batch = cfg["dims"], cfg["batch"]
-    form = pac.PAC_FORM_F64 if args.form == "f64" else pac.PAC_FORM_F32
+    form = FORMS[args.form]
     tdt = torch.float64 if form == pac.PAC_FORM_F64 else torch.float32
     dev = torch.device("cuda", 0)
     L = pac.load()
@@ -779,9 +782,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--config", choices=sorted(CONFIGS), default="c3")
-    ap.add_argument("--form", choices=["f64", "f32"], default="f64")
+    ap.add_argument("--form", choices=sorted(FORMS), default="f64")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
-    ap.add_argument("--no-forms", action="store_true", help="skip the FP32 comparison")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="skip the FP32 and tensor-core form comparison")
     ap.add_argument("--l2", choices=["on", "off"], default="on",
                     help="keep the output (the passes' intermediate) L2-persisting")
     ap.add_argument("--profile", action="store_true",
@@ -821,16 +825,19 @@ def main():
     out = run_ours(args, world, dist)
     out["e2e"] = run_e2e(args, world, dist)
     if not args.no_forms and args.form == "f64":
-        a32 = argparse.Namespace(**vars(args))
-        a32.form = "f32"
-        o32 = run_ours(a32, world, dist)
         out["forms"] = {
             "f64": {"value": out["value"], "rel_l2_vs_numpy_fp64": out["rel_l2_vs_numpy_fp64"],
-                    "roofline_frac": out["roofline"]["frac"]},
-            "f32": {"value": o32["value"], "rel_l2_vs_numpy_fp64": o32["rel_l2_vs_numpy_fp64"],
-                    "speedup_vs_f64": round(o32["value"] / out["value"], 3),
-                    "roofline_frac": o32["roofline"]["frac"],
-                    "passes": o32["roofline"]["passes"]}}
+                    "max_err_vs_numpy_fp64": out["max_err_vs_numpy_fp64"],
+                    "roofline_frac": out["roofline"]["frac"]}}
+        for fm in ("f32", "tc"):
+            af = argparse.Namespace(**vars(args))
+            af.form = fm
+            of = run_ours(af, world, dist)
+            out["forms"][fm] = {
+                "value": of["value"], "rel_l2_vs_numpy_fp64": of["rel_l2_vs_numpy_fp64"],
+                "max_err_vs_numpy_fp64": of["max_err_vs_numpy_fp64"],
+                "speedup_vs_f64": round(of["value"] / out["value"], 3),
+                "roofline_frac": of["roofline"]["frac"], "passes": of["roofline"]["passes"]}
     if rank == 0 and world == 1 and not args.no_cpu:
         procs = min(os.cpu_count() or 1, 16)
         pool = CpuPool(args.config, procs)

@@ -26,7 +26,7 @@ LIB = os.path.join(HERE, "lib", "libpac.so")
 LIB_EMU = os.path.join(HERE, "lib", "libpac_emu.so")
 
 PAC_SUCCESS = 0
-PAC_FORM_F64, PAC_FORM_F32 = 0, 1
+PAC_FORM_F64, PAC_FORM_F32, PAC_FORM_TC = 0, 1, 2
 OP_AT, OP_A, OP_CONJ_A, OP_FFT, OP_IFFT, OP_UFFT, OP_UIFFT = range(7)
 
 _lock = threading.Lock()

@@ -62,10 +62,11 @@ long long be_launch_count();
 // i belongs to descriptor k = item_desc[i] and is CTA i - starts[k] of that
 // pass.  descs (ndesc), starts (ndesc + 1) and item_desc (total) live in
 // device memory; smem is the largest shared-memory size of the passes.
-int be_queue_prepare(int elem_bytes, int b2, size_t smem);  // outside graph capture
+// tc = 1: the tensor-core form's kernel (PassDesc.tc set in every descriptor).
+int be_queue_prepare(int elem_bytes, int b2, int tc, size_t smem);  // outside graph capture
 int be_launch_queue(const PassDesc* descs, const long long* starts, const int* item_desc,
                     int ndesc, long long total, unsigned long long* counter, int elem_bytes,
-                    int b2, size_t smem, void* stream);
+                    int b2, int tc, size_t smem, void* stream);
 // CUDA graphs: capture what a thread issues on `stream` between begin and
 // end, then replay it.  be_graph_supported() is 0 where nothing can be
 // captured (the host replay), and callers then issue the work directly.

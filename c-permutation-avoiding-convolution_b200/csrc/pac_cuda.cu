@@ -51,7 +51,7 @@ static int cuda_fail(cudaError_t e, const char* what) {
 // ---------------------------------------------------------------------------
 // kernels
 // ---------------------------------------------------------------------------
-template <typename T, int B2>
+template <typename T, int B2, int TC>
 __global__ void __launch_bounds__(256) pac_pass_kernel(const PassDesc d) {
   extern __shared__ __align__(16) unsigned char pac_smem[];
   __shared__ long long s_lb[128];
@@ -69,16 +69,17 @@ __global__ void __launch_bounds__(256) pac_pass_kernel(const PassDesc d) {
     }
   }
   __syncthreads();
-  pass_body<T, B2>(d, cta, sre, sim, s_lb, s_lb + 64);
+  pass_body<T, B2, TC>(d, cta, sre, sim, s_lb, s_lb + 64);
 }
 
 // A pass compiled for one geometry (pac_special.h): tile W = 2^LOGW lines of
 // 2^LOGL elements, NT threads, register bound for MINB CTAs per SM.
-template <typename T, int B2, int MODE, int SIGN, int LOGL, int COLS, int LOGW, int NT, int MINB>
+template <typename T, int B2, int MODE, int SIGN, int LOGL, int COLS, int LOGW, int NT, int MINB,
+          int TC>
 __global__ void __launch_bounds__(NT, MINB) pac_special_kernel(const PassDesc d) {
   constexpr int W = 1 << LOGW;
-  constexpr int PITCH = pitch_for((int)sizeof(T), LOGL, W, COLS);
-  using SP = Shape<LOGL, LOGW, PITCH, COLS>;
+  constexpr int PITCH = pitch_for((int)sizeof(T), LOGL, W, COLS, TC);
+  using SP = Shape<LOGL, LOGW, PITCH, COLS, TC>;
   extern __shared__ __align__(16) unsigned char pac_smem[];
   __shared__ long long s_lb[W];
   T* sre = reinterpret_cast<T*>(pac_smem);
@@ -86,7 +87,7 @@ __global__ void __launch_bounds__(NT, MINB) pac_special_kernel(const PassDesc d)
   const long long cta = blockIdx.x;
   if ((int)threadIdx.x < W) s_lb[threadIdx.x] = line_base(d, cta * W + threadIdx.x);
   __syncthreads();
-  pass_body_ct<T, B2, MODE, SIGN, SP, NT, RadsFor<LOGL, B2>>(d, cta, sre, sim, s_lb, s_lb);
+  pass_body_ct<T, B2, MODE, SIGN, SP, NT, RadsFor<LOGL, B2>, TC>(d, cta, sre, sim, s_lb, s_lb);
 }
 
 // Persistent CTAs over a device work queue (many passes of different
@@ -95,7 +96,7 @@ __global__ void __launch_bounds__(NT, MINB) pac_special_kernel(const PassDesc d)
 // is copied into shared memory (unless the CTA's previous item had the same
 // pass) and the CTA runs that pass's CTA `item - starts[k]` with the
 // run-time geometry of pac_pass_kernel.
-template <typename T, int B2>
+template <typename T, int B2, int TC>
 __global__ void __launch_bounds__(256) pac_queue_kernel(const PassDesc* __restrict__ descs,
                                                         const long long* __restrict__ starts,
                                                         const int* __restrict__ item_desc,
@@ -135,7 +136,7 @@ __global__ void __launch_bounds__(256) pac_queue_kernel(const PassDesc* __restri
       s_lb[64 + threadIdx.x] = s_lb[threadIdx.x];
     }
     __syncthreads();
-    pass_body<T, B2>(sd, cta, sre, sim, s_lb, s_lb + 64);
+    pass_body<T, B2, TC>(sd, cta, sre, sim, s_lb, s_lb + 64);
     __syncthreads();  // sd, s_lb and the tile are reused by the next item
   }
 }
@@ -573,14 +574,14 @@ int be_stream_wait(void* waiter, void* waitee) {
   return PAC_SUCCESS;
 }
 
-template <typename T, int B2>
+template <typename T, int B2, int TC = 0>
 static int launch_pass_t(const PassDesc& d, long long grid, int threads, size_t smem,
                          void* stream) {
   // opt the kernel into the device's whole shared-memory budget once per
   // device, so that every pass geometry (<= 200 KiB) launches
   static std::mutex mu;
   static std::set<int> configured;
-  auto kern = pac_pass_kernel<T, B2>;
+  auto kern = pac_pass_kernel<T, B2, TC>;
   if (smem > 48 * 1024) {
     int dev = 0;
     cudaGetDevice(&dev);
@@ -634,15 +635,15 @@ static int launch_special(const PassDesc& d, int elem_bytes, int b2, long long g
                           size_t smem, void* stream, bool* done) {
   *done = false;
   const int cols = d.logS > 0 ? 1 : 0;
-#define PAC_X(T, BY, B2_, MO, SG, LL, CO, LW, NT_, MB)                                        \
+#define PAC_X(T, BY, B2_, MO, SG, LL, CO, LW, NT_, MB, TC_)                                   \
   if (!*done && elem_bytes == BY && b2 == B2_ && d.mode == MO &&                           \
       (MO == MODE_CONV || d.sign == SG) && d.logL == LL && cols == CO && d.W == (1 << LW) && \
-      threads == NT_) {                                                                    \
+      threads == NT_ && d.tc == TC_) {                                                     \
     static std::mutex mu;                                                                  \
     static std::set<int> configured;                                                       \
     *done = true;                                                                          \
-    return launch_kernel(pac_special_kernel<T, B2_, MO, SG, LL, CO, LW, NT_, MB>, d, grid,  \
-                         threads, smem, stream, configured, mu);                           \
+    return launch_kernel(pac_special_kernel<T, B2_, MO, SG, LL, CO, LW, NT_, MB, TC_>, d,   \
+                         grid, threads, smem, stream, configured, mu);                     \
   }
   PAC_SPECIAL_LIST(PAC_X)
 #undef PAC_X
@@ -696,11 +697,11 @@ static int launch_cluster(const PassDesc& d, int elem_bytes, int b2, long long g
 // ---------------------------------------------------------------------------
 // work-queue launches and graphs (pac_multi.cpp)
 // ---------------------------------------------------------------------------
-template <typename T, int B2>
+template <typename T, int B2, int TC = 0>
 static int queue_prepare_t(size_t smem, int* grid_per_sm) {
   static std::mutex mu;
   static std::set<int> configured;
-  auto kern = pac_queue_kernel<T, B2>;
+  auto kern = pac_queue_kernel<T, B2, TC>;
   int dev = 0;
   PAC_CU(cudaGetDevice(&dev), "cudaGetDevice");
   {
@@ -727,7 +728,11 @@ static int queue_prepare_t(size_t smem, int* grid_per_sm) {
   return PAC_SUCCESS;
 }
 
-static int queue_prepare(int elem_bytes, int b2, size_t smem, int* grid_per_sm) {
+static int queue_prepare(int elem_bytes, int b2, int tc, size_t smem, int* grid_per_sm) {
+  if (tc && b2 != 3) {  // (base-8 schedules have no radix-16 stage)
+    if (b2 == 1) return queue_prepare_t<float, 1, 1>(smem, grid_per_sm);
+    return queue_prepare_t<float, 2, 1>(smem, grid_per_sm);
+  }
   if (elem_bytes == 8) {
     if (b2 == 1) return queue_prepare_t<double, 1>(smem, grid_per_sm);
     if (b2 == 2) return queue_prepare_t<double, 2>(smem, grid_per_sm);
@@ -738,31 +743,34 @@ static int queue_prepare(int elem_bytes, int b2, size_t smem, int* grid_per_sm) 
   return queue_prepare_t<float, 3>(smem, grid_per_sm);
 }
 
-int be_queue_prepare(int elem_bytes, int b2, size_t smem) {
-  return queue_prepare(elem_bytes, b2, smem, nullptr);
+int be_queue_prepare(int elem_bytes, int b2, int tc, size_t smem) {
+  return queue_prepare(elem_bytes, b2, tc, smem, nullptr);
 }
 
 int be_launch_queue(const PassDesc* descs, const long long* starts, const int* item_desc,
                     int ndesc, long long total, unsigned long long* counter, int elem_bytes,
-                    int b2, size_t smem, void* stream) {
+                    int b2, int tc, size_t smem, void* stream) {
   (void)ndesc;
   if (total <= 0) return PAC_SUCCESS;
   int per_sm = 0;
-  PAC_TRY_BE(queue_prepare(elem_bytes, b2, smem, &per_sm));
+  PAC_TRY_BE(queue_prepare(elem_bytes, b2, tc, smem, &per_sm));
   long long grid = (long long)per_sm * be_num_sms();
   if (grid > total) grid = total;
   cudaStream_t s = (cudaStream_t)stream;
-#define PAC_Q(T, B)                                                                        \
-  pac_queue_kernel<T, B><<<(unsigned)grid, 256, smem, s>>>(descs, starts, item_desc, total, \
-                                                             counter)
-  if (elem_bytes == 8) {
-    if (b2 == 1) PAC_Q(double, 1);
-    else if (b2 == 2) PAC_Q(double, 2);
-    else PAC_Q(double, 3);
+#define PAC_Q(T, B, TC_)                                                                \
+  pac_queue_kernel<T, B, TC_><<<(unsigned)grid, 256, smem, s>>>(descs, starts, item_desc, \
+                                                                  total, counter)
+  if (tc && b2 != 3) {
+    if (b2 == 1) PAC_Q(float, 1, 1);
+    else PAC_Q(float, 2, 1);
+  } else if (elem_bytes == 8) {
+    if (b2 == 1) PAC_Q(double, 1, 0);
+    else if (b2 == 2) PAC_Q(double, 2, 0);
+    else PAC_Q(double, 3, 0);
   } else {
-    if (b2 == 1) PAC_Q(float, 1);
-    else if (b2 == 2) PAC_Q(float, 2);
-    else PAC_Q(float, 3);
+    if (b2 == 1) PAC_Q(float, 1, 0);
+    else if (b2 == 2) PAC_Q(float, 2, 0);
+    else PAC_Q(float, 3, 0);
   }
 #undef PAC_Q
   PAC_CU(cudaGetLastError(), "pac_queue_kernel launch");
@@ -876,6 +884,13 @@ int be_launch_pass(const PassDesc& d, int elem_bytes, int b2, long long grid, in
   if (d.spec) {
     bool done = false;
     return launch_special(d, elem_bytes, b2, grid, threads, smem, stream, &done);
+  }
+  if (d.tc) {
+    // tensor-core form: FP32 storage, radix-16 stages (digit bases 2 and 4;
+    // base-8 schedules have no radix-16 stage)
+    if (b2 == 1) return launch_pass_t<float, 1, 1>(d, grid, threads, smem, stream);
+    if (b2 == 2) return launch_pass_t<float, 2, 1>(d, grid, threads, smem, stream);
+    return launch_pass_t<float, 3>(d, grid, threads, smem, stream);
   }
   if (elem_bytes == 8) {
     if (b2 == 1) return launch_pass_t<double, 1>(d, grid, threads, smem, stream);

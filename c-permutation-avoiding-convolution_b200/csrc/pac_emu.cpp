@@ -65,7 +65,7 @@ int be_event_elapsed(void*, void*, float* ms) {
   return PAC_SUCCESS;
 }
 
-template <typename T, int B2>
+template <typename T, int B2, int TC = 0>
 static void replay(const PassDesc& d, long long grid) {
   std::vector<T> sm((size_t)2 * d.W * d.pitch);
   std::vector<long long> lb(128);
@@ -75,24 +75,23 @@ static void replay(const PassDesc& d, long long grid) {
       if (d.nat) nat_line<B2>(d, g, &lb[w], &lb[64 + w]);
       else lb[w] = lb[64 + w] = line_base(d, g);
     }
-    pass_body<T, B2>(d, cta, sm.data(), sm.data() + (size_t)d.W * d.pitch, lb.data(),
-                     lb.data() + 64);
+    pass_body<T, B2, TC>(d, cta, sm.data(), sm.data() + (size_t)d.W * d.pitch, lb.data(),
+                         lb.data() + 64);
   }
 }
 
 // replay of a specialised kernel (pac_special.h): the compile-time body
-template <typename T, int B2, int MODE, int SIGN, int LOGL, int COLS, int LOGW, int NT>
+template <typename T, int B2, int MODE, int SIGN, int LOGL, int COLS, int LOGW, int NT, int TC>
 static void replay_special(const PassDesc& d, long long grid) {
   constexpr int W = 1 << LOGW;
-  constexpr int PITCH = pitch_for((int)sizeof(T), LOGL, W, COLS);
-  using SP = Shape<LOGL, LOGW, PITCH, COLS>;
+  constexpr int PITCH = pitch_for((int)sizeof(T), LOGL, W, COLS, TC);
+  using SP = Shape<LOGL, LOGW, PITCH, COLS, TC>;
   std::vector<T> sm((size_t)2 * W * PITCH);
   std::vector<long long> lb(W);
   for (long long cta = 0; cta < grid; ++cta) {
     for (int w = 0; w < W; ++w) lb[w] = line_base(d, cta * W + w);
-    pass_body_ct<T, B2, MODE, SIGN, SP, NT, RadsFor<LOGL, B2>>(d, cta, sm.data(),
-                                                               sm.data() + (size_t)W * PITCH,
-                                                               lb.data(), lb.data());
+    pass_body_ct<T, B2, MODE, SIGN, SP, NT, RadsFor<LOGL, B2>, TC>(
+        d, cta, sm.data(), sm.data() + (size_t)W * PITCH, lb.data(), lb.data());
   }
 }
 
@@ -206,10 +205,10 @@ int be_launch_pass(const PassDesc& d, int elem_bytes, int b2, long long grid, in
   }
   if (d.spec) {
     const int cols = d.logS > 0 ? 1 : 0;
-#define PAC_X(T, BY, B2_, MO, SG, LL, CO, LW, NT_, MB)                                        \
+#define PAC_X(T, BY, B2_, MO, SG, LL, CO, LW, NT_, MB, TC_)                                   \
   if (elem_bytes == BY && b2 == B2_ && d.mode == MO && (MO == MODE_CONV || d.sign == SG) && \
-      d.logL == LL && cols == CO && d.W == (1 << LW) && threads == NT_) {                  \
-    replay_special<T, B2_, MO, SG, LL, CO, LW, NT_>(d, grid);                              \
+      d.logL == LL && cols == CO && d.W == (1 << LW) && threads == NT_ && d.tc == TC_) {   \
+    replay_special<T, B2_, MO, SG, LL, CO, LW, NT_, TC_>(d, grid);                              \
     g_launches++;                                                                          \
     return PAC_SUCCESS;                                                                    \
   }
@@ -218,7 +217,10 @@ int be_launch_pass(const PassDesc& d, int elem_bytes, int b2, long long grid, in
     return set_error(PAC_ERROR_INTERNAL, "no specialised replay for a pass marked special");
   }
   if (d.W > 64) return set_error(PAC_ERROR_INTERNAL, "W > 64");
-  if (elem_bytes == 8) {
+  if (d.tc && b2 != 3) {
+    if (b2 == 1) replay<float, 1, 1>(d, grid);
+    else replay<float, 2, 1>(d, grid);
+  } else if (elem_bytes == 8) {
     if (b2 == 1) replay<double, 1>(d, grid);
     else if (b2 == 2) replay<double, 2>(d, grid);
     else replay<double, 3>(d, grid);
@@ -386,7 +388,7 @@ long long be_launch_count() { return g_launches.load(); }
 
 // work-queue launch: the items in queue order, one CTA each (the queue's
 // order is the one a single persistent CTA would take)
-template <typename T, int B2>
+template <typename T, int B2, int TC = 0>
 static void replay_queue(const PassDesc* descs, const long long* starts, const int* item_desc,
                          long long total) {
   std::vector<long long> lb(128);
@@ -396,17 +398,20 @@ static void replay_queue(const PassDesc* descs, const long long* starts, const i
     const long long cta = it - starts[k];
     std::vector<T> sm((size_t)2 * d.W * d.pitch, std::numeric_limits<T>::quiet_NaN());
     for (int w = 0; w < d.W; ++w) lb[w] = lb[64 + w] = line_base(d, cta * d.W + w);
-    pass_body<T, B2>(d, cta, sm.data(), sm.data() + (size_t)d.W * d.pitch, lb.data(),
-                     lb.data() + 64);
+    pass_body<T, B2, TC>(d, cta, sm.data(), sm.data() + (size_t)d.W * d.pitch, lb.data(),
+                         lb.data() + 64);
   }
 }
 
-int be_queue_prepare(int, int, size_t) { return PAC_SUCCESS; }
+int be_queue_prepare(int, int, int, size_t) { return PAC_SUCCESS; }
 
 int be_launch_queue(const PassDesc* descs, const long long* starts, const int* item_desc, int,
-                    long long total, unsigned long long* counter, int elem_bytes, int b2, size_t,
-                    void*) {
-  if (elem_bytes == 8) {
+                    long long total, unsigned long long* counter, int elem_bytes, int b2, int tc,
+                    size_t, void*) {
+  if (tc && b2 != 3) {
+    if (b2 == 1) replay_queue<float, 1, 1>(descs, starts, item_desc, total);
+    else replay_queue<float, 2, 1>(descs, starts, item_desc, total);
+  } else if (elem_bytes == 8) {
     if (b2 == 1) replay_queue<double, 1>(descs, starts, item_desc, total);
     else if (b2 == 2) replay_queue<double, 2>(descs, starts, item_desc, total);
     else replay_queue<double, 3>(descs, starts, item_desc, total);

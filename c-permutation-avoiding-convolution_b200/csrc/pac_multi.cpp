@@ -60,6 +60,7 @@ struct pac_multi_s {
   int nprob = 0;
   int bytes = 8;
   int b2 = 1;
+  int tc = 0;  // tensor-core form
   std::vector<long long> off;       // nprob + 1
   std::vector<int> shape_of;        // problem -> plan index
   std::vector<pac_plan_t> plans;    // one per distinct shape
@@ -178,7 +179,7 @@ static int build_levels(pac_multi_s* m, const void* x_re, const void* x_im, cons
   // the host staging vector dies here: wait for the copy
   PAC_TRY(be_stream_sync(stream));
   for (auto& groups : m->levels)
-    for (auto& G : groups) PAC_TRY(be_queue_prepare(m->bytes, m->b2, G.smem));
+    for (auto& G : groups) PAC_TRY(be_queue_prepare(m->bytes, m->b2, m->tc, G.smem));
   if (!m->side) PAC_TRY(be_stream_create(&m->side));
   return PAC_SUCCESS;
 }
@@ -187,7 +188,7 @@ static int launch_group(pac_multi_s* m, const Group& G, unsigned long long* cnt,
   char* dev = (char*)m->dev;
   return be_launch_queue((const PassDesc*)(dev + G.desc_off),
                          (const long long*)(dev + G.start_off), (const int*)(dev + G.item_off),
-                         G.ndesc, G.total, cnt, m->bytes, m->b2, G.smem, stream);
+                         G.ndesc, G.total, cnt, m->bytes, m->b2, m->tc, G.smem, stream);
 }
 
 // counters to zero, then every level: its groups side by side (the second
@@ -253,6 +254,7 @@ PAC_API int pac_multi_create(pac_multi_t* multi, int nprob, const int* ranks, co
   std::unique_ptr<pac_multi_s> m(new pac_multi_s());
   m->nprob = nprob;
   m->b2 = b2;
+  m->tc = form == PAC_FORM_TC;
   m->off.assign(nprob + 1, 0);
   m->shape_of.assign(nprob, 0);
   std::map<std::vector<int>, int> seen;

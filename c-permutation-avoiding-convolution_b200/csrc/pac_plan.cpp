@@ -72,6 +72,7 @@ struct VAx {
 struct Schedule {
   int bytes = 8;  // element bytes of one real component
   int b2 = 1;     // log2 of the digit base
+  int tc = 0;     // tensor-core form: radix-16 stages on the tensor cores
   std::vector<VAx> vax;
   std::vector<std::vector<int>> rad;  // per factor: stage radix logs, DIF order
   void* pool = nullptr;               // stage twiddle tables
@@ -260,6 +261,7 @@ static PassSpec make_pass(const Schedule& s, int vi, long long batch, long long 
   d.logW = 0;
   while ((1 << d.logW) < d.W) ++d.logW;
   d.pitch = pitch_for(esz, v.log, d.W);
+  d.tc = s.tc;
   const std::vector<int>& rad = s.rad[vi];
   d.nst = (int)rad.size();
   int logK = v.log;
@@ -307,7 +309,8 @@ static void apply_special(const Schedule& s, PassSpec& p) {
   // column pass whose tile a CTA cluster shares (W columns within the
   // stride, whole tiles), opt-in: PAC_CLUSTER_VARIANT=k picks the k-th
   // candidate geometry of the cluster list
-  const char* cvar = getenv("PAC_CLUSTER_VARIANT");
+  // (the cluster and pipelined variants have no tensor-core stages)
+  const char* cvar = d.tc ? nullptr : getenv("PAC_CLUSTER_VARIANT");
   if (d.logS > 0 && cvar != nullptr) {
     int logC = 0;
     if (cluster_geometry(s.bytes, p.b2, d.mode, d.sign, d.logL, &logW, &logC, &nt, atoi(cvar)) &&
@@ -327,7 +330,7 @@ static void apply_special(const Schedule& s, PassSpec& p) {
   // pipelined column pass, opt-in (PAC_PIPE=1): persistent CTAs, one per
   // SM, tensor-copy prefetch of the next tile (16-byte aligned input arrays
   // for the tensor maps)
-  const char* pipe = getenv("PAC_PIPE");
+  const char* pipe = d.tc ? nullptr : getenv("PAC_PIPE");
   if (d.logS > 0 && cvar == nullptr && pipe != nullptr && atoi(pipe) != 0 &&
       pipe_geometry(s.bytes, p.b2, d.mode, d.sign, d.logL, &logW, &nt) && logW <= d.logS &&
       (d.nlines & ((1LL << logW) - 1)) == 0 && (d.nlines >> d.logS) < (1LL << 31) &&
@@ -347,16 +350,16 @@ static void apply_special(const Schedule& s, PassSpec& p) {
   }
   const char* var = getenv("PAC_SPECIAL_VARIANT");
   const int variant = var ? atoi(var) : 0;
-  if (!special_geometry(s.bytes, p.b2, d.mode, d.sign, d.logL, d.logS > 0 ? 1 : 0, &logW, &nt,
-                        variant) &&
-      !special_geometry(s.bytes, p.b2, d.mode, d.sign, d.logL, d.logS > 0 ? 1 : 0, &logW, &nt))
+  const int cols = d.logS > 0 ? 1 : 0;
+  if (!special_geometry(s.bytes, p.b2, d.mode, d.sign, d.logL, cols, d.tc, &logW, &nt, variant) &&
+      !special_geometry(s.bytes, p.b2, d.mode, d.sign, d.logL, cols, d.tc, &logW, &nt))
     return;
   const long long W = 1LL << logW;
   if ((d.nlines & (W - 1)) != 0) return;
   if (d.logS > 0 && logW > d.logS) return;
   d.W = (int)W;
   d.logW = logW;
-  d.pitch = pitch_for(s.bytes, d.logL, d.W, d.logS > 0 ? 1 : 0);
+  d.pitch = pitch_for(s.bytes, d.logL, d.W, cols, d.tc);
   d.nthreads = nt;
   d.spec = 1;
   p.threads = nt;
@@ -725,7 +728,7 @@ PAC_API int pac_plan_create_axes(pac_plan_t* plan, int rank, const int* dims,
       return set_error(PAC_ERROR_UNSUPPORTED_RADIX,
                        "pac_plan_create: digit base %d (axis %d) not in {2,4,8}", base, a);
   }
-  if (form != PAC_FORM_F64 && form != PAC_FORM_F32)
+  if (form != PAC_FORM_F64 && form != PAC_FORM_F32 && form != PAC_FORM_TC)
     return set_error(PAC_ERROR_INVALID_VALUE, "pac_plan_create: unknown form %d", form);
   int st = be_init();
   if (st != PAC_SUCCESS) return st;
@@ -751,6 +754,7 @@ PAC_API int pac_plan_create_axes(pac_plan_t* plan, int rank, const int* dims,
   int bytes = form == PAC_FORM_F64 ? 8 : 4;
   st = build_schedule(p->main, rank, p->logs, b2s, bytes);
   if (st != PAC_SUCCESS) return st;
+  p->main.tc = form == PAC_FORM_TC;
   if (bytes != 8) {
     p->s64.reset(new Schedule());
     st = build_schedule(*p->s64, rank, p->logs, b2s, 8);

@@ -18,26 +18,31 @@ namespace pac {
 // pitch_for are defined with the stage engine, pac_stages.cuh)
 
 // fields: element type, bytes, log2 digit base, mode, sign (DIF/DIT), log2 L,
-// column tile (element stride > 1), log2 W, threads, min CTAs per SM
+// column tile (element stride > 1), log2 W, threads, min CTAs per SM,
+// tensor-core form (radix-16 stages on the tensor cores, pac_tc.cuh)
 #define PAC_SPECIAL_LIST(X)                                \
-  X(double, 8, 1, MODE_CONV, 0, 11, 0, 0, 128, 4)          \
-  X(double, 8, 1, MODE_DIF, -1, 11, 1, 2, 512, 1)          \
-  X(double, 8, 1, MODE_DIT, +1, 11, 1, 2, 512, 1)          \
-  X(float, 4, 1, MODE_CONV, 0, 11, 0, 1, 256, 2)           \
-  X(float, 4, 1, MODE_DIF, -1, 11, 1, 3, 512, 1)           \
-  X(float, 4, 1, MODE_DIT, +1, 11, 1, 3, 512, 1)           \
-  X(double, 8, 1, MODE_DIF, -1, 11, 1, 1, 256, 2)          \
-  X(double, 8, 1, MODE_DIT, +1, 11, 1, 1, 256, 2)          \
-  X(float, 4, 1, MODE_DIF, -1, 11, 1, 2, 512, 1)           \
-  X(float, 4, 1, MODE_DIT, +1, 11, 1, 2, 512, 1)           \
+  X(double, 8, 1, MODE_CONV, 0, 11, 0, 0, 128, 4, 0)          \
+  X(double, 8, 1, MODE_DIF, -1, 11, 1, 2, 512, 1, 0)          \
+  X(double, 8, 1, MODE_DIT, +1, 11, 1, 2, 512, 1, 0)          \
+  X(float, 4, 1, MODE_CONV, 0, 11, 0, 1, 256, 2, 0)           \
+  X(float, 4, 1, MODE_DIF, -1, 11, 1, 3, 512, 1, 0)           \
+  X(float, 4, 1, MODE_DIT, +1, 11, 1, 3, 512, 1, 0)           \
+  X(double, 8, 1, MODE_DIF, -1, 11, 1, 1, 256, 2, 0)          \
+  X(double, 8, 1, MODE_DIT, +1, 11, 1, 1, 256, 2, 0)          \
+  X(float, 4, 1, MODE_DIF, -1, 11, 1, 2, 512, 1, 0)           \
+  X(float, 4, 1, MODE_DIT, +1, 11, 1, 2, 512, 1, 0)           \
   /* 3D FP32: 256-point rows and columns (256^3, and the middle axis of */ \
   /* 512 x 256 x 128), 512-point columns and 128-point rows */           \
-  X(float, 4, 1, MODE_CONV, 0, 8, 0, 4, 256, 2)            \
-  X(float, 4, 1, MODE_DIF, -1, 8, 1, 4, 256, 2)            \
-  X(float, 4, 1, MODE_DIT, +1, 8, 1, 4, 256, 2)            \
-  X(float, 4, 1, MODE_DIF, -1, 9, 1, 4, 512, 1)            \
-  X(float, 4, 1, MODE_DIT, +1, 9, 1, 4, 512, 1)            \
-  X(float, 4, 1, MODE_CONV, 0, 7, 0, 5, 256, 2)
+  X(float, 4, 1, MODE_CONV, 0, 8, 0, 4, 256, 2, 0)            \
+  X(float, 4, 1, MODE_DIF, -1, 8, 1, 4, 256, 2, 0)            \
+  X(float, 4, 1, MODE_DIT, +1, 8, 1, 4, 256, 2, 0)            \
+  X(float, 4, 1, MODE_DIF, -1, 9, 1, 4, 512, 1, 0)            \
+  X(float, 4, 1, MODE_DIT, +1, 9, 1, 4, 512, 1, 0)            \
+  X(float, 4, 1, MODE_CONV, 0, 7, 0, 5, 256, 2, 0)            \
+  /* tensor-core form, 2048-point rows and 8-line columns */             \
+  X(float, 4, 1, MODE_CONV, 0, 11, 0, 1, 256, 2, 1)           \
+  X(float, 4, 1, MODE_DIF, -1, 11, 1, 3, 512, 1, 1)           \
+  X(float, 4, 1, MODE_DIT, +1, 11, 1, 3, 512, 1, 1)
 // Measured on C3 (2048^2): FP64 columns W=4 (32-byte rows) 53 us vs W=2
 // 68 us; FP32 columns W=8 34 us vs W=4 45 us -- row width, not occupancy,
 // bounds these passes.  On 3D 512 x 256 x 128 FP32 the specialised passes
@@ -113,12 +118,12 @@ inline bool cluster_geometry(int bytes, int b2, int mode, int sign, int logL, in
   return false;
 }
 
-inline bool special_geometry(int bytes, int b2, int mode, int sign, int logL, int cols,
+inline bool special_geometry(int bytes, int b2, int mode, int sign, int logL, int cols, int tc,
                              int* logW, int* nt, int variant = 0) {
   int seen = 0;
-#define PAC_X(T, BY, B2_, MO, SG, LL, CO, LW, NT_, MB)                                    \
+#define PAC_X(T, BY, B2_, MO, SG, LL, CO, LW, NT_, MB, TC_)                               \
   if (bytes == BY && b2 == B2_ && mode == MO && (MO == MODE_CONV || sign == SG) &&     \
-      logL == LL && cols == CO && seen++ == variant) {                                 \
+      logL == LL && cols == CO && tc == TC_ && seen++ == variant) {                    \
     *logW = LW;                                                                        \
     *nt = NT_;                                                                         \
     return true;                                                                       \

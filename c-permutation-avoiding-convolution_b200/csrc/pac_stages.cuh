@@ -28,8 +28,10 @@ enum { IO_SMEM = 0, IO_GLOBAL = 1 };
 PAC_HDC bool col_pad32(int bytes, int cols, int W) { return bytes == 4 && cols == 1 && W == 8; }
 PAC_HD int sidx_col32(int e) { return e + (e >> 3) + 8 * (e >> 7); }
 
-// geometry policy; -1 = read from the PassDesc at run time
-template <int LOGL_ = -1, int LOGW_ = -1, int PITCH_ = -1, int COLS_ = -1>
+// geometry policy; -1 = read from the PassDesc at run time.  TCL_ = 1: a
+// tile of the tensor-core form, whose column tiles keep the one-per-32 pad
+// (pitch_for gives them an odd pitch instead of sidx_col32)
+template <int LOGL_ = -1, int LOGW_ = -1, int PITCH_ = -1, int COLS_ = -1, int TCL_ = 0>
 struct Shape {
   static constexpr int kLogL = LOGL_;
   static constexpr int kLogW = LOGW_;
@@ -61,7 +63,7 @@ struct Shape {
   // shared-memory index of element e of line w: padded lines
   template <typename T>
   static PAC_HD int sm(const PassDesc& d, int w, int e) {
-    if constexpr (col_pad32((int)sizeof(T), COLS_, LOGW_ >= 0 ? 1 << LOGW_ : 0))
+    if constexpr (!TCL_ && col_pad32((int)sizeof(T), COLS_, LOGW_ >= 0 ? 1 << LOGW_ : 0))
       return w * pitch(d) + sidx_col32(e);
     else
       return w * pitch(d) + sidx<T>(e);
@@ -279,6 +281,10 @@ PAC_HD void middle_bf(const PassDesc& d, T* sre, T* sim, int src, int dst, int u
   });
 }
 
+}  // namespace pac
+#include "pac_tc.cuh"
+namespace pac {
+
 // ---------------------------------------------------------------------------
 // Phases: a loop over butterflies; the device runs it with one butterfly per
 // thread, the host emulator with a plain loop.  Barriers separate a phase
@@ -343,6 +349,26 @@ PAC_HD void middle_dispatch(const PassDesc& d, T* sre, T* sim, int logR, int src
   }
 }
 
+// Tensor-core form (PassDesc.tc; the generic kernels are instantiated with
+// TC = 1 for it): radix-16 stages of FP32 passes run on the tensor cores
+// (stage_tc); every other stage and the convolution middle stay on the CUDA
+// cores.
+template <typename T, int TC>
+PAC_HD bool tc_stage(int logR) {
+  return TC && sizeof(T) == 4 && logR == 4;
+}
+template <typename T, int B2, bool DIF>
+PAC_HD void stage_tc_rt(const PassDesc& d, long long cta, T* sre, T* sim, int logK, int twoff,
+                        int sign, int src, int dst, int nbf, const long long* lbi,
+                        const long long* lbo) {
+  if constexpr (sizeof(T) == 4 && B2 != 3) {
+    if (sign < 0)
+      stage_tc<B2, -1, DIF, RtShape, -1>(d, cta, sre, sim, logK, twoff, src, dst, nbf, lbi, lbo);
+    else
+      stage_tc<B2, +1, DIF, RtShape, -1>(d, cta, sre, sim, logK, twoff, src, dst, nbf, lbi, lbo);
+  }
+}
+
 // block size (log) of stage i of the DIF order: L / (R_0 ... R_{i-1})
 PAC_HD int stage_logK(const PassDesc& d, int i) {
   int logK = d.logL;
@@ -350,7 +376,7 @@ PAC_HD int stage_logK(const PassDesc& d, int i) {
   return logK;
 }
 
-template <typename T, int B2>
+template <typename T, int B2, int TC = 0>
 PAC_HD void pass_body(const PassDesc& d, long long cta, T* sre, T* sim, const long long* lbi,
                       const long long* lbo) {
   const bool nat = d.nat != 0;
@@ -362,6 +388,11 @@ PAC_HD void pass_body(const PassDesc& d, long long cta, T* sre, T* sim, const lo
       int dst = (i == nst - 1 && !nat) ? IO_GLOBAL : IO_SMEM;
       int nbf = d.W << (d.logL - logR);
       if (i > 0) PAC_SYNC();
+      if (tc_stage<T, TC>(logR)) {
+        stage_tc_rt<T, B2, true>(d, cta, sre, sim, logK, d.tw_off[i], d.sign, src, dst, nbf, lbi,
+                                 lbo);
+        continue;
+      }
       PAC_FOR_BF(nbf, u) {
         stage_dispatch<T, B2, true>(d, cta, sre, sim, logK, logR, d.tw_off[i], d.sign, src, dst, u,
                                     lbi, lbo);
@@ -404,6 +435,11 @@ PAC_HD void pass_body(const PassDesc& d, long long cta, T* sre, T* sim, const lo
       int dst = (k == nst - 1) ? IO_GLOBAL : IO_SMEM;
       int nbf = d.W << (d.logL - logR);
       if (k > 0) PAC_SYNC();
+      if (tc_stage<T, TC>(logR)) {
+        stage_tc_rt<T, B2, false>(d, cta, sre, sim, logK, d.tw_off[i], d.sign, src, dst, nbf, lbi,
+                                  lbo);
+        continue;
+      }
       PAC_FOR_BF(nbf, u) {
         stage_dispatch<T, B2, false>(d, cta, sre, sim, logK, logR, d.tw_off[i], d.sign, src, dst,
                                      u, lbi, lbo);
@@ -415,6 +451,11 @@ PAC_HD void pass_body(const PassDesc& d, long long cta, T* sre, T* sim, const lo
       int src = (i == 0) ? IO_GLOBAL : IO_SMEM;
       int nbf = d.W << (d.logL - logR);
       if (i > 0) PAC_SYNC();
+      if (tc_stage<T, TC>(logR)) {
+        stage_tc_rt<T, B2, true>(d, cta, sre, sim, logK, d.tw_off[i], -1, src, IO_SMEM, nbf, lbi,
+                                 lbo);
+        continue;
+      }
       PAC_FOR_BF(nbf, u) {
         stage_dispatch<T, B2, true>(d, cta, sre, sim, logK, logR, d.tw_off[i], -1, src, IO_SMEM,
                                     u, lbi, lbo);
@@ -433,6 +474,11 @@ PAC_HD void pass_body(const PassDesc& d, long long cta, T* sre, T* sim, const lo
       int dst = (i == 0) ? IO_GLOBAL : IO_SMEM;
       int nbf = d.W << (d.logL - logR);
       PAC_SYNC();
+      if (tc_stage<T, TC>(logR)) {
+        stage_tc_rt<T, B2, false>(d, cta, sre, sim, logK, d.tw_off[i], +1, IO_SMEM, dst, nbf, lbi,
+                                  lbo);
+        continue;
+      }
       PAC_FOR_BF(nbf, u) {
         stage_dispatch<T, B2, false>(d, cta, sre, sim, logK, logR, d.tw_off[i], +1, IO_SMEM, dst,
                                      u, lbi, lbo);
@@ -465,9 +511,10 @@ struct Rads {
 #define PAC_FOR_BF_CT(n, NT, u) for (int u = 0; u < (n); ++u)
 #endif
 
-template <typename T, int B2, int MODE, int SIGN, class SP, int NT, class RS>
+template <typename T, int B2, int MODE, int SIGN, class SP, int NT, class RS, int TC = 0>
 PAC_HD void pass_body_ct(const PassDesc& d, long long cta, T* sre, T* sim, const long long* lbi,
                          const long long* lbo) {
+  static_assert(!TC || sizeof(T) == 4, "the tensor-core form stores FP32");
   constexpr int GIO = IO_GLOBAL;
   constexpr int LOGL = SP::kLogL;
   constexpr int LOGW = SP::kLogW;
@@ -480,10 +527,16 @@ PAC_HD void pass_body_ct(const PassDesc& d, long long cta, T* sre, T* sim, const
       constexpr int LRr = RS::v[i];
       constexpr int nbf = 1 << (LOGW + LOGL - LRr);
       if constexpr (i > 0) PAC_SYNC();
-      PAC_FOR_BF_CT(nbf, NT, u) {
-        stage_bf<T, B2, (1 << LRr), SIGN, true, SP, LK>(
-            d, cta, sre, sim, LK, d.tw_off[i], i == 0 ? GIO : IO_SMEM,
-            i == n - 1 ? GIO : IO_SMEM, u, lbi, lbo);
+      if constexpr (TC && LRr == 4) {
+        stage_tc<B2, SIGN, true, SP, LK>(d, cta, sre, sim, LK, d.tw_off[i],
+                                         i == 0 ? GIO : IO_SMEM, i == n - 1 ? GIO : IO_SMEM, nbf,
+                                         lbi, lbo);
+      } else {
+        PAC_FOR_BF_CT(nbf, NT, u) {
+          stage_bf<T, B2, (1 << LRr), SIGN, true, SP, LK>(
+              d, cta, sre, sim, LK, d.tw_off[i], i == 0 ? GIO : IO_SMEM,
+              i == n - 1 ? GIO : IO_SMEM, u, lbi, lbo);
+        }
       }
     });
   } else if constexpr (MODE == MODE_DIT) {
@@ -494,10 +547,16 @@ PAC_HD void pass_body_ct(const PassDesc& d, long long cta, T* sre, T* sim, const
       constexpr int LRr = RS::v[i];
       constexpr int nbf = 1 << (LOGW + LOGL - LRr);
       if constexpr (k > 0) PAC_SYNC();
-      PAC_FOR_BF_CT(nbf, NT, u) {
-        stage_bf<T, B2, (1 << LRr), SIGN, false, SP, LK>(
-            d, cta, sre, sim, LK, d.tw_off[i], k == 0 ? GIO : IO_SMEM,
-            k == n - 1 ? GIO : IO_SMEM, u, lbi, lbo);
+      if constexpr (TC && LRr == 4) {
+        stage_tc<B2, SIGN, false, SP, LK>(d, cta, sre, sim, LK, d.tw_off[i],
+                                          k == 0 ? GIO : IO_SMEM, k == n - 1 ? GIO : IO_SMEM, nbf,
+                                          lbi, lbo);
+      } else {
+        PAC_FOR_BF_CT(nbf, NT, u) {
+          stage_bf<T, B2, (1 << LRr), SIGN, false, SP, LK>(
+              d, cta, sre, sim, LK, d.tw_off[i], k == 0 ? GIO : IO_SMEM,
+              k == n - 1 ? GIO : IO_SMEM, u, lbi, lbo);
+        }
       }
     });
   } else {
@@ -507,9 +566,14 @@ PAC_HD void pass_body_ct(const PassDesc& d, long long cta, T* sre, T* sim, const
       constexpr int LRr = RS::v[i];
       constexpr int nbf = 1 << (LOGW + LOGL - LRr);
       if constexpr (i > 0) PAC_SYNC();
-      PAC_FOR_BF_CT(nbf, NT, u) {
-        stage_bf<T, B2, (1 << LRr), -1, true, SP, LK>(
-            d, cta, sre, sim, LK, d.tw_off[i], i == 0 ? GIO : IO_SMEM, IO_SMEM, u, lbi, lbo);
+      if constexpr (TC && LRr == 4) {
+        stage_tc<B2, -1, true, SP, LK>(d, cta, sre, sim, LK, d.tw_off[i], i == 0 ? GIO : IO_SMEM,
+                                       IO_SMEM, nbf, lbi, lbo);
+      } else {
+        PAC_FOR_BF_CT(nbf, NT, u) {
+          stage_bf<T, B2, (1 << LRr), -1, true, SP, LK>(
+              d, cta, sre, sim, LK, d.tw_off[i], i == 0 ? GIO : IO_SMEM, IO_SMEM, u, lbi, lbo);
+        }
       }
     });
     {
@@ -525,9 +589,14 @@ PAC_HD void pass_body_ct(const PassDesc& d, long long cta, T* sre, T* sim, const
       constexpr int LRr = RS::v[i];
       constexpr int nbf = 1 << (LOGW + LOGL - LRr);
       PAC_SYNC();
-      PAC_FOR_BF_CT(nbf, NT, u) {
-        stage_bf<T, B2, (1 << LRr), +1, false, SP, LK>(
-            d, cta, sre, sim, LK, d.tw_off[i], IO_SMEM, i == 0 ? GIO : IO_SMEM, u, lbi, lbo);
+      if constexpr (TC && LRr == 4) {
+        stage_tc<B2, +1, false, SP, LK>(d, cta, sre, sim, LK, d.tw_off[i], IO_SMEM,
+                                        i == 0 ? GIO : IO_SMEM, nbf, lbi, lbo);
+      } else {
+        PAC_FOR_BF_CT(nbf, NT, u) {
+          stage_bf<T, B2, (1 << LRr), +1, false, SP, LK>(
+              d, cta, sre, sim, LK, d.tw_off[i], IO_SMEM, i == 0 ? GIO : IO_SMEM, u, lbi, lbo);
+        }
       }
     });
   }
@@ -722,10 +791,16 @@ using RadsFor = typename RadsImpl<LG, B2, std::make_integer_sequence<int, sched_
 // shared-memory line pitch: one pad element every 16 (FP64) / 32 (FP32)
 // (FP32 8-line column tiles: sidx_col32), then skewed so that the W lines
 // of a column tile start in different banks
-PAC_HDC int pitch_for(int bytes, int logL, int W, int cols = 0) {
+PAC_HDC int pitch_for(int bytes, int logL, int W, int cols = 0, int tc = 0) {
   const int L = 1 << logL;
   const int SH = bytes == 8 ? 4 : 5, NB = bytes == 8 ? 16 : 32;
-  int pitch = col_pad32(bytes, cols, W) ? L + (L >> 3) + 8 * (L >> 7) : L + (L >> SH);
+  if (tc && cols && W > 1) {
+    // tensor-core column tiles: one pad per 32 and an odd pitch, so that the
+    // 8 lines x 4 slots of a tile load or store fall on distinct banks
+    const int p = L + (L >> SH);
+    return p + ((1 - p % NB) % NB + NB) % NB;
+  }
+  int pitch = !tc && col_pad32(bytes, cols, W) ? L + (L >> 3) + 8 * (L >> 7) : L + (L >> SH);
   if (W > 1) {
     int want = (NB / (W < NB ? W : NB)) % NB;
     pitch += ((want - pitch % NB) % NB + NB) % NB;

@@ -20,7 +20,11 @@
  *
  * Forms: PAC_FORM_F64 computes and stores complex FP64.  PAC_FORM_F32 stores
  * and computes FP32, with twiddles and the filter spectrum computed in FP64
- * on the device and rounded once.
+ * on the device and rounded once.  PAC_FORM_TC is PAC_FORM_F32 with every
+ * radix-16 stage run on the tensor cores: dense 16 x 16 complex DFT products
+ * on split hi + lo FP16 operands (three products, FP32 accumulation, a
+ * power-of-two scale per butterfly); the other stages, the twiddles and the
+ * filter product stay FP32 on the CUDA cores.
  *
  * Threading: plans are immutable after creation; calls on one plan from
  * several host threads are safe when they use distinct buffers (the plan's
@@ -60,7 +64,7 @@ enum {
 };
 
 /* storage / compute forms */
-enum { PAC_FORM_F64 = 0, PAC_FORM_F32 = 1 };
+enum { PAC_FORM_F64 = 0, PAC_FORM_F32 = 1, PAC_FORM_TC = 2 };
 
 /* transform operators (per axis, all axes of the plan) */
 enum {

@@ -9,6 +9,7 @@ from conftest import O, pac, rel_l2, rng
 
 TOL = 1e-13  # FP64 forms vs the FP64 oracle (north star: 1e-13 relative L2)
 TOL_F32 = 1e-6  # FP32 form vs the FP64 oracle
+TOL_TC = 1e-6  # tensor-core form (split FP16 radix-16 stages) vs the FP64 oracle
 
 OPS = ((O.OP_A, "A"), (O.OP_CONJ, "conjA"), (O.OP_AT, "At"))
 KINDS = ("fft", "fft2", "ufft", "ifft", "uifft")
@@ -215,7 +216,7 @@ def check_multi(L, shapes, form, stream=False, seed=3):
     FFT convolution; a second call (the CUDA-graph replay when a stream is
     given) repeats the first bit for bit."""
     dt = np.float64 if form == pac.PAC_FORM_F64 else np.float32
-    tol = TOL if form == pac.PAC_FORM_F64 else TOL_F32
+    tol = TOL if form == pac.PAC_FORM_F64 else TOL_TC if form == pac.PAC_FORM_TC else TOL_F32
     g = rng(seed)
     m = pac.MultiPlan(L, shapes, 2, form)
     off = m.offsets
@@ -310,3 +311,35 @@ def check_axis_bases(L, dims, bases, form, batch=2):
     pac.check(L, L.pac_plan_get_info(plan.h, C.byref(info)), "info")
     plan.close()
     assert list(info.digit_bases[:len(dims)]) == list(bases)
+
+
+def max_rel(a, b):
+    """Largest elementwise error relative to the largest reference magnitude."""
+    return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+
+
+def check_tc(L, orc, dims, batch, base, seed=5, ops=True):
+    """Tensor-core form: convolution against numpy's FP64 FFT convolution and
+    the transform operators against the oracle's butterflies; returns the
+    relative L2 and max errors of every result."""
+    g = rng(seed)
+    shape = (batch,) + tuple(dims)
+    x = g.uniform(-1, 1, shape) + 1j * g.uniform(-1, 1, shape)
+    h = g.standard_normal(dims) + 1j * g.standard_normal(dims)
+    y = native_conv(L, dims, batch, base, pac.PAC_FORM_TC, x, h)
+    z = fftconv(x, h[None], tuple(range(1, len(shape))))
+    errs = {"conv": (crel(y, z), max_rel(y, z))}
+    if ops:
+        for op, oop in ((pac.OP_AT, O.OP_AT), (pac.OP_CONJ_A, O.OP_CONJ)):
+            y = native_transform(L, dims, batch, base, pac.PAC_FORM_TC, op, x)
+            for b in range(batch):
+                zr, zi = orc.butterflies(oop, base, x[b].real, x[b].imag)
+                z = zr + 1j * zi
+                e = errs.get(op, (0.0, 0.0))
+                errs[op] = (max(e[0], crel(y[b], z)), max(e[1], max_rel(y[b], z)))
+        y = native_transform(L, dims, batch, base, pac.PAC_FORM_TC, pac.OP_FFT, x)
+        z = np.fft.fftn(x, axes=tuple(range(1, len(shape))))
+        errs[pac.OP_FFT] = (crel(y, z), max_rel(y, z))
+    for k, (l2, mx) in errs.items():
+        assert l2 < TOL_TC, (dims, base, k, l2, mx)
+    return errs

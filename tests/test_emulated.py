@@ -191,3 +191,39 @@ def test_multi_uneven_batch(emu, form):
 def test_axis_bases(emu, dims, bases, form):
     """One digit base per axis (pac_plan_create_axes)."""
     P.check_axis_bases(emu, dims, bases, form)
+
+
+# Tensor-core form: the lane code of the split-FP16 radix-16 stages replayed
+# lane by lane around an MMA modelled from the PTX fragment layouts.
+# Shapes: the specialised 2048-point row (CONV) and 8-line column kernels,
+# generic radix-16 stages of base 2 and 4, 3D, and 16-point lines whose
+# stages have fewer butterflies than a 16-butterfly tile.
+@pytest.mark.parametrize("dims,batch,base", [
+    ((64, 2048), 1, 2), ((2048, 64), 1, 2), ((4096,), 3, 4), ((4096,), 2, 2),
+    ((16, 16, 256), 1, 2), ((16, 16), 5, 2), ((16, 16), 3, 4)])
+def test_tc_form(emu, orc, dims, batch, base):
+    errs = P.check_tc(emu, orc, dims, batch, base, ops=int(np.prod(dims)) <= 2 ** 14)
+    # the radix-16 stages are on the tensor cores: the error is of the split
+    # FP16 products, well above an FP64 path's and at most a few FP32 ulps,
+    # and the result is not the FP32 form's
+    assert errs["conv"][0] > 1e-12
+    g = rng(5)
+    shape = (batch,) + dims
+    x = g.uniform(-1, 1, shape) + 1j * g.uniform(-1, 1, shape)
+    h = g.standard_normal(dims) + 1j * g.standard_normal(dims)
+    y_tc = P.native_conv(emu, dims, batch, base, pac.PAC_FORM_TC, x, h)
+    y_32 = P.native_conv(emu, dims, batch, base, pac.PAC_FORM_F32, x, h)
+    assert not np.array_equal(y_tc, y_32)
+
+
+def test_tc_form_split_axes(emu, orc, monkeypatch):
+    """4-step twiddles on tensor-core stages: 2^16 as 256 x 256 factors
+    (radix-16 stages next to the 4-step twiddle, DIF post and DIT pre)."""
+    monkeypatch.setenv("PAC_MAX_FACTOR_LOG", "8")
+    P.check_tc(emu, orc, (2 ** 16,), 1, 2, ops=True)
+    P.check_tc(emu, orc, (256, 1024), 1, 4, ops=False)
+
+
+def test_tc_multi(emu):
+    shapes = [(256,), (2048, 16), (16, 16, 16), (4096,), (2,)]
+    P.check_multi(emu, shapes, pac.PAC_FORM_TC)

@@ -60,14 +60,14 @@ def test_c1_against_reference_and_direct_sum(lib, orc):
         assert rel_l2(y[0], y[1], *d) < P.TOL
 
 
-@pytest.mark.parametrize("form", [pac.PAC_FORM_F64, pac.PAC_FORM_F32])
+@pytest.mark.parametrize("form", [pac.PAC_FORM_F64, pac.PAC_FORM_F32, pac.PAC_FORM_TC])
 def test_c2_batched_1d(lib, orc, form):
     """C2: 1024 x 2^16 with one 257-tap filter; sampled rows against the
     oracle (reference radix 4, 2^16 = 4^8) and the whole batch through
     linearity: sum_b (x_b * h) = (sum_b x_b) * h."""
     x, h = W.c2()
     y = P.native_conv(lib, (65536,), 1024, 2, form, x, h)
-    tol = P.TOL if form == pac.PAC_FORM_F64 else P.TOL_F32
+    tol = {pac.PAC_FORM_F64: P.TOL, pac.PAC_FORM_F32: P.TOL_F32, pac.PAC_FORM_TC: P.TOL_TC}[form]
     for b in (0, 1, 511, 1023):
         z = orc.convolution(O.METHOD_PAC, 4, x[b].real, x[b].imag, h.real, h.imag)
         assert P.crel(y[b], z[0] + 1j * z[1]) < tol
@@ -76,13 +76,13 @@ def test_c2_batched_1d(lib, orc, form):
     assert P.crel(y.sum(axis=0), z[0] + 1j * z[1]) < tol * 4
 
 
-@pytest.mark.parametrize("form", [pac.PAC_FORM_F64, pac.PAC_FORM_F32])
+@pytest.mark.parametrize("form", [pac.PAC_FORM_F64, pac.PAC_FORM_F32, pac.PAC_FORM_TC])
 def test_c3_2d(lib, orc, form):
     """C3: 2048^2, Gaussian 31x31 filter; oracle at reference radix 2."""
     x, h = W.c3()
     y = P.native_conv(lib, (2048, 2048), 1, 2, form, x, h)[0]
     z = orc.convolution(O.METHOD_PAC, 2, x.real, x.imag, h.real, h.imag)
-    tol = P.TOL if form == pac.PAC_FORM_F64 else P.TOL_F32
+    tol = {pac.PAC_FORM_F64: P.TOL, pac.PAC_FORM_F32: P.TOL_F32, pac.PAC_FORM_TC: P.TOL_TC}[form]
     assert P.crel(y, z[0] + 1j * z[1]) < tol
 
 
@@ -248,3 +248,49 @@ def test_axis_bases(lib, dims, bases, form):
     """One digit base per axis: 512 x 256 x 128 at bases 8, 4, 2 (the
     reference runs it at radix 2 only)."""
     P.check_axis_bases(lib, dims, bases, form, batch=1 if np.prod(dims) > 2 ** 20 else 2)
+
+
+# Tensor-core form (mma.sync m16n8k16, split FP16 operands): the same shapes
+# as the host replay's test, against the FP64 oracle, and against the host
+# replay of the same lane code (an MMA modelled from the PTX fragment
+# layouts): the two differ only by the MMA's FP32 accumulation order.
+@pytest.mark.parametrize("dims,batch,base", [
+    ((64, 2048), 1, 2), ((2048, 64), 1, 2), ((4096,), 3, 4), ((4096,), 2, 2),
+    ((16, 16, 256), 1, 2), ((16, 16), 5, 2), ((16, 16), 3, 4), ((2048, 2048), 1, 2)])
+def test_tc_form(lib, emu, orc, dims, batch, base):
+    big = int(np.prod(dims)) > 2 ** 20
+    P.check_tc(lib, orc, dims, batch, base, ops=not big)
+    if big:
+        return
+    g = rng(9)
+    shape = (batch,) + dims
+    x = g.uniform(-1, 1, shape) + 1j * g.uniform(-1, 1, shape)
+    h = g.standard_normal(dims) + 1j * g.standard_normal(dims)
+    y = P.native_conv(lib, dims, batch, base, pac.PAC_FORM_TC, x, h)
+    e = P.native_conv(emu, dims, batch, base, pac.PAC_FORM_TC, x, h)
+    assert P.crel(y, e) < 2e-7
+    y32 = P.native_conv(lib, dims, batch, base, pac.PAC_FORM_F32, x, h)
+    assert not np.array_equal(y, y32)
+
+
+def test_tc_form_split_axes(lib, orc, monkeypatch):
+    monkeypatch.setenv("PAC_MAX_FACTOR_LOG", "8")
+    P.check_tc(lib, orc, (2 ** 16,), 1, 2, ops=True)
+    P.check_tc(lib, orc, (256, 1024), 1, 4, ops=False)
+
+
+@pytest.mark.parametrize("stream", [False, True])
+def test_tc_multi(lib, stream):
+    shapes = [(256,), (2048, 16), (16, 16, 16), (4096,), (2,), (2048, 2048)]
+    P.check_multi(lib, shapes, pac.PAC_FORM_TC, stream=stream)
+
+
+@pytest.mark.parametrize("shape", [(256, 256, 256), (512, 256, 128)])
+def test_c4_3d_tc(lib, shape):
+    g = rng(12)
+    x = g.uniform(-1, 1, shape) + 1j * g.uniform(-1, 1, shape)
+    h = np.zeros(shape, np.complex128)
+    h[:8, :8, :8] = g.standard_normal((8, 8, 8))
+    y = P.native_conv(lib, shape, 1, 2, pac.PAC_FORM_TC, x, h)[0]
+    z = P.fftconv(x, h, (0, 1, 2))
+    assert P.crel(y, z) < P.TOL_TC
