@@ -36,6 +36,8 @@ int be_launch_pass(const PassDesc& d, int elem_bytes, int b2, long long grid, in
                    size_t smem, void* stream);
 // stage table (K = 2^logK, R = 2^logR): entry j*(R-1) + s-1 = w_K^{j s}, forward sign
 int be_fill_stage_tw(void* dst, int elem_bytes, int logK, int logR, void* stream);
+// the tensor-core form's DFT operand table: TC_CONST_SETS x 32 TcConst
+int be_fill_tc_const(void* dst, void* stream);
 // dst[k] = w_N^{k * stride} for k < count, N = 2^logN, forward sign
 int be_fill_pow_tw(void* dst, int elem_bytes, long long count, long long stride, int logN,
                    void* stream);

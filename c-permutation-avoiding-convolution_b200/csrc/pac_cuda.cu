@@ -908,6 +908,17 @@ int be_launch_pass(const PassDesc& d, int elem_bytes, int b2, long long grid, in
     g_launches.fetch_add(1);                \
   } while (0)
 
+__global__ void fill_tc_const_kernel(TcConst* t) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < TC_CONST_SETS * 32) tc_const_fill(i >> 5, i & 31, t[i]);
+}
+
+int be_fill_tc_const(void* dst, void* stream) {
+  fill_tc_const_kernel<<<TC_CONST_SETS, 32, 0, (cudaStream_t)stream>>>((TcConst*)dst);
+  PAC_LAUNCHED("fill_tc_const");
+  return PAC_SUCCESS;
+}
+
 int be_fill_stage_tw(void* dst, int elem_bytes, int logK, int logR, void* stream) {
   long long n = (1LL << (logK - logR)) * ((1LL << logR) - 1);
   if (elem_bytes == 8)

@@ -247,6 +247,13 @@ static void put(void* dst, long long i, double c, double s) {
   p[2 * i + 1] = (T)s;
 }
 
+int be_fill_tc_const(void* dst, void*) {
+  TcConst* t = (TcConst*)dst;
+  for (int set = 0; set < TC_CONST_SETS; ++set)
+    for (int lane = 0; lane < 32; ++lane) tc_const_fill(set, lane, t[set * 32 + lane]);
+  return PAC_SUCCESS;
+}
+
 int be_fill_stage_tw(void* dst, int elem_bytes, int logK, int logR, void*) {
   long long R1 = (1LL << logR) - 1, K = 1LL << logK;
   long long n = (K >> logR) * R1;

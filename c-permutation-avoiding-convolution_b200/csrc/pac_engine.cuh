@@ -93,8 +93,10 @@ struct PassDesc {
   // 1: pipelined column pass, one persistent CTA per SM with tensor-copy
   // prefetch of the next tile (pac_special.h, PAC_PIPE_LIST; ColPipe)
   int pipe;
-  // 1: tensor-core form, radix-16 stages on the tensor cores (pac_tc.cuh)
+  // 1: tensor-core form, radix-16 stages on the tensor cores (pac_tc.cuh);
+  // tcc: their DFT operands, per stage kind and lane (tc_const_set)
   int tc;
+  const void* tcc;
 };
 
 // ---------------------------------------------------------------------------

@@ -73,6 +73,7 @@ struct Schedule {
   int bytes = 8;  // element bytes of one real component
   int b2 = 1;     // log2 of the digit base
   int tc = 0;     // tensor-core form: radix-16 stages on the tensor cores
+  void* tcc = nullptr;  // its DFT operand table (tensor-core form)
   std::vector<VAx> vax;
   std::vector<std::vector<int>> rad;  // per factor: stage radix logs, DIF order
   void* pool = nullptr;               // stage twiddle tables
@@ -85,6 +86,7 @@ struct Schedule {
   std::map<int, Tw4> tw4;  // keyed by log N
   ~Schedule() {
     if (pool) be_free(pool);
+    if (tcc) be_free(tcc);
     for (auto& kv : tw4) {
       be_free(kv.second.lo);
       be_free(kv.second.hi);
@@ -262,6 +264,7 @@ static PassSpec make_pass(const Schedule& s, int vi, long long batch, long long 
   while ((1 << d.logW) < d.W) ++d.logW;
   d.pitch = pitch_for(esz, v.log, d.W);
   d.tc = s.tc;
+  d.tcc = s.tcc;
   const std::vector<int>& rad = s.rad[vi];
   d.nst = (int)rad.size();
   int logK = v.log;
@@ -755,6 +758,11 @@ PAC_API int pac_plan_create_axes(pac_plan_t* plan, int rank, const int* dims,
   st = build_schedule(p->main, rank, p->logs, b2s, bytes);
   if (st != PAC_SUCCESS) return st;
   p->main.tc = form == PAC_FORM_TC;
+  if (p->main.tc) {
+    st = be_malloc(&p->main.tcc, sizeof(TcConst) * TC_CONST_SETS * 32);
+    if (st == PAC_SUCCESS) st = be_fill_tc_const(p->main.tcc, nullptr);
+    if (st != PAC_SUCCESS) return st;
+  }
   if (bytes != 8) {
     p->s64.reset(new Schedule());
     st = build_schedule(*p->s64, rank, p->logs, b2s, 8);

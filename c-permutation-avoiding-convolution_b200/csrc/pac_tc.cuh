@@ -205,6 +205,57 @@ PAC_HD void tc_const(int lane, bool useq, TcConst& wc) {
   }
 }
 
+// The operands of every stage kind, built once per plan by tc_const into a
+// device table (PassDesc.tcc, be_fill_tc_const): set (digit base 2 or 4,
+// sign, DIF/DIT, slot map) x 32 lanes.  A stage loads its lane's 96 bytes
+// instead of rebuilding them.
+enum { TC_CONST_SETS = 16 };
+PAC_HDC int tc_const_set(int b2, int sign, bool dif, bool useq) {
+  return (((b2 - 1) * 2 + (sign > 0 ? 1 : 0)) * 2 + (dif ? 1 : 0)) * 2 + (useq ? 1 : 0);
+}
+// inverse of tc_const_set: fill entry `set` of the table for `lane`
+PAC_HD void tc_const_fill(int set, int lane, TcConst& wc) {
+  const bool useq = set & 1, dif = (set >> 1) & 1, pos = (set >> 2) & 1;
+  const int b2 = (set >> 3) + 1;
+  if (b2 == 1) {
+    if (pos) dif ? tc_const<1, +1, true>(lane, useq, wc) : tc_const<1, +1, false>(lane, useq, wc);
+    else dif ? tc_const<1, -1, true>(lane, useq, wc) : tc_const<1, -1, false>(lane, useq, wc);
+  } else {
+    if (pos) dif ? tc_const<2, +1, true>(lane, useq, wc) : tc_const<2, +1, false>(lane, useq, wc);
+    else dif ? tc_const<2, -1, true>(lane, useq, wc) : tc_const<2, -1, false>(lane, useq, wc);
+  }
+}
+PAC_HD void tc_const_load(const PassDesc& d, int set, int lane, TcConst& wc) {
+  const TcConst* p = (const TcConst*)d.tcc + set * 32 + lane;
+#if defined(__CUDA_ARCH__)
+  static_assert(sizeof(TcConst) == 96, "6 x 16 bytes, one per member");
+  const uint4* v = reinterpret_cast<const uint4*>(p);
+  auto put = [](uint32_t(&m)[2][2], uint4 x) {
+    m[0][0] = x.x;
+    m[0][1] = x.y;
+    m[1][0] = x.z;
+    m[1][1] = x.w;
+  };
+  put(wc.rh, __ldg(v + 0));
+  put(wc.rl, __ldg(v + 1));
+  put(wc.ih, __ldg(v + 2));
+  put(wc.il, __ldg(v + 3));
+  put(wc.nh, __ldg(v + 4));
+  put(wc.nl, __ldg(v + 5));
+#else
+  wc = *p;
+#endif
+}
+
+// Shared-memory offset of the element ell * s past a butterfly's first
+// element e0, for lines padded one element per 32 (sidx<float>, the layout
+// of every tensor-core tile): sidx(e0 + ell s) = sidx(e0) + tc_soff(ell s),
+// because e0 mod 32 + (ell s) mod 32 < 32 for the butterflies of a
+// radix-16 stage: e0 = blk * 16 ell + j with j < ell; for ell >= 32 the
+// second term is 0; for 2 <= ell < 32, e0 mod 32 = j <= ell - 1 and
+// (ell s) mod 32 <= 32 - ell; for ell = 1, e0 mod 32 is 0 or 16 and s <= 15.
+PAC_HD int tc_soff(int x) { return x + (x >> 5); }
+
 // Per-lane state of one tile: butterflies g (bh = 0) and g + 8 (bh = 1).
 struct TcLane {
   float xr[2][4], xi[2][4];  // inputs k = 2q + (kk & 1) + 8 (kk >> 1), kk = 0..3
@@ -213,6 +264,7 @@ struct TcLane {
   uint32_t arh[4], arl[4], aih[4], ail[4];  // A registers: reg = bh + 2 * (kk >> 1)
   float yr[2][4], yi[2][4];  // D registers of column half h
   int w[2], e0[2], j[2];
+  int sb[2];  // shared-memory index of the butterfly's first element
   bool ok[2];
 };
 
@@ -237,6 +289,7 @@ PAC_HD void tc_load(const PassDesc& d, long long cta, const float* sre, const fl
     t.w[bh] = w;
     t.j[bh] = j;
     t.e0[bh] = e0;
+    t.sb[bh] = SP::template sm<float>(d, w, e0);
     float mx = 0.f;
     for (int kk = 0; kk < 4; ++kk) {
       const int s = tc_slot(2 * q + (kk & 1) + 8 * (kk >> 1), useq);
@@ -247,7 +300,7 @@ PAC_HD void tc_load(const PassDesc& d, long long cta, const float* sre, const fl
           const long long gi = lbi[w] + ((long long)e << d.logS);
           v = Cx<float>{ld_g(ire + gi), ld_g(iim + gi)};
         } else {
-          const int si = SP::template sm<float>(d, w, e);
+          const int si = t.sb[bh] + tc_soff(ell * s);
           v = Cx<float>{sre[si], sim[si]};
         }
         if constexpr (!DIF) {
@@ -313,7 +366,7 @@ PAC_HD void tc_store(const PassDesc& d, long long cta, float* sre, float* sim, i
         ore[gi] = v.re;
         oim[gi] = v.im;
       } else {
-        const int si = SP::template sm<float>(d, w, e);
+        const int si = t.sb[bh] + tc_soff(ell * s);
         sre[si] = v.re;
         sim[si] = v.im;
       }
@@ -422,7 +475,7 @@ PAC_HD void stage_tc(const PassDesc& d, long long cta, float* sre, float* sim, i
 #if defined(__CUDA_ARCH__)
   const int lane = (int)threadIdx.x & 31;
   TcConst wc;
-  tc_const<B2, SIGN, DIF>(lane, useq, wc);
+  tc_const_load(d, tc_const_set(B2, SIGN, DIF, useq), lane, wc);
   for (int tile = (int)threadIdx.x >> 5; tile < ntiles; tile += (int)blockDim.x >> 5) {
     TcLane t;
     tc_load<B2, SIGN, DIF, SP>(d, cta, sre, sim, logK, twoff, src, dst, lane, tile, nbf, lbi, t);
@@ -437,7 +490,8 @@ PAC_HD void stage_tc(const PassDesc& d, long long cta, float* sre, float* sim, i
   }
 #else
   TcConst wc[32];
-  for (int lane = 0; lane < 32; ++lane) tc_const<B2, SIGN, DIF>(lane, useq, wc[lane]);
+  for (int lane = 0; lane < 32; ++lane)
+    tc_const_load(d, tc_const_set(B2, SIGN, DIF, useq), lane, wc[lane]);
   for (int tile = 0; tile < ntiles; ++tile) {
     TcLane t[32];
     for (int lane = 0; lane < 32; ++lane)
