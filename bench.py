@@ -26,6 +26,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -285,7 +286,8 @@ def run_ours(args, world, dist):
     l2_bytes = ybuf.numel() * ybuf.element_size() if args.l2 == "on" else 0
     if l2_bytes:
         pac.check(L, L.pac_stream_set_l2_persisting(sp, ybuf.data_ptr(), l2_bytes), "l2")
-    plan = pac.Plan(L, dims, batch, 2, form)
+    tuned = tune_workload(L, args, dims, batch, form, sp)
+    plan = pac.Plan(L, dims, batch, 2, form)  # the tuned knobs, through PAC_TUNE_CACHE
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     plan.filter_spectrum(hd[0].data_ptr(), hd[1].data_ptr(), Hh[0].data_ptr(), Hh[1].data_ptr(),
@@ -389,6 +391,7 @@ def run_ours(args, world, dist):
            "filter_spectrum_ms": round(spectrum_ms, 4), "rel_l2_vs_numpy_fp64": max(errs),
            "max_err_vs_numpy_fp64": max(maxs)}
     out["config"]["l2_persisting_output"] = bool(l2_bytes)
+    out["config"]["autotune"] = tuned
     if l2_bytes:
         pac.check(L, L.pac_stream_set_l2_persisting(sp, None, 0), "l2")
     plan.close()
@@ -433,6 +436,21 @@ def run_profile(args):
     plan.close()
     return {"mode": "profile", "config": args.config, "form": args.form,
             "ms_per_step": ev0.elapsed_time(ev1) / max(args.steps, 1)}
+
+
+def _tune_record(r):
+    return {"knobs": r.tune.as_dict(), "ms": round(r.ms, 5), "default_ms": round(r.default_ms, 5),
+            "candidates": r.candidates, "cached": bool(r.cached),
+            "cache": os.environ.get("PAC_TUNE_CACHE")}
+
+
+def tune_workload(L, args, dims, batch, form, sp):
+    """pac_autotune for the workload (before anything is timed); the result
+    lands in PAC_TUNE_CACHE, which every plan this process creates reads."""
+    if args.tune != "on":
+        return None
+    return _tune_record(pac.autotune(L, dims, batch, 2, form, stream=sp,
+                                     cache=os.environ["PAC_TUNE_CACHE"]))
 
 
 def run_e2e(args, world, dist):
@@ -568,14 +586,21 @@ def run_c5(args, world, dist):
     dev = torch.device("cuda", local)
     L = pac.load()
     shapes = W.c5_shapes()
-    m = pac.MultiPlan(L, shapes, 2, pac.PAC_FORM_F32)
+    stream = torch.cuda.Stream(dev)  # graph capture needs a non-legacy stream
+    sp = stream.cuda_stream
+    tuned = None
+    if args.tune == "on":
+        r = pac.multi_autotune(L, shapes, 2, pac.PAC_FORM_F32, stream=sp,
+                               cache=os.environ["PAC_TUNE_CACHE"])
+        tuned = _tune_record(r)
+        m = pac.MultiPlan(L, shapes, 2, pac.PAC_FORM_F32, tune=r.tune)
+    else:
+        m = pac.MultiPlan(L, shapes, 2, pac.PAC_FORM_F32)
     offs = m.offsets
     n = int(offs[-1])
     x, h = _c5_inputs(torch, dev, shapes, offs)
     H = [torch.empty(n, dtype=torch.float32, device=dev) for _ in range(2)]
     y = [torch.empty(n, dtype=torch.float32, device=dev) for _ in range(2)]
-    stream = torch.cuda.Stream(dev)  # graph capture needs a non-legacy stream
-    sp = stream.cuda_stream
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     ev0.record(stream)
@@ -658,6 +683,7 @@ def run_c5(args, world, dist):
                       "shapes": info["nshapes"], "elements": n, "form": "f32",
                       "digit_base": 2, "levels": info["nlevels"],
                       "work_items_per_level": info["items"], "cuda_graph": bool(info["graph"]),
+                      "autotune": tuned,
                       "l2": f"inputs larger than L2: {n * 8 / 2**30:.1f} GiB per packed array",
                       "parallelism": f"replicas x{world}"},
            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
@@ -786,6 +812,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--no-forms", action="store_true",
                     help="skip the FP32 and tensor-core form comparison")
+    ap.add_argument("--tune", choices=["on", "off"], default="on",
+                    help="autotune the plan knobs (pac_autotune) before timing; the cache is "
+                         "PAC_TUNE_CACHE if set, else a fresh file for this run")
     ap.add_argument("--l2", choices=["on", "off"], default="on",
                     help="keep the output (the passes' intermediate) L2-persisting")
     ap.add_argument("--profile", action="store_true",
@@ -793,6 +822,11 @@ def main():
                          "(two input buffers, no clock soak, e2e, CPU or FP32 legs)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
+    if args.profile:
+        args.tune = "off"  # ncu captures count launches: no tuning runs before them
+    if args.tune == "on" and not os.environ.get("PAC_TUNE_CACHE"):
+        os.environ["PAC_TUNE_CACHE"] = os.path.join(tempfile.mkdtemp(prefix="pac_tune_"),
+                                                    "tune.jsonl")
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if args.profile:

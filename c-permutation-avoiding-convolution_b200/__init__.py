@@ -62,6 +62,14 @@ def _declare(L):
     L.pac_plan_create.argtypes = [C.POINTER(_vp), i, C.POINTER(i), i, i, i]
     L.pac_plan_create_axes.argtypes = [C.POINTER(_vp), i, C.POINTER(i), C.POINTER(i), i, i]
     L.pac_plan_get_info.argtypes = [_vp, C.POINTER(PlanInfo)]
+    L.pac_plan_create_tuned.argtypes = [C.POINTER(_vp), i, C.POINTER(i), C.POINTER(i), i, i,
+                                        C.POINTER(Tune)]
+    L.pac_autotune.argtypes = [i, C.POINTER(i), C.POINTER(i), i, i, _vp, C.c_char_p,
+                               C.POINTER(TuneResult)]
+    L.pac_multi_create_tuned.argtypes = [C.POINTER(_vp), i, C.POINTER(i), C.POINTER(i), i, i,
+                                         C.POINTER(Tune)]
+    L.pac_multi_autotune.argtypes = [i, C.POINTER(i), C.POINTER(i), i, i, _vp, C.c_char_p,
+                                     C.POINTER(TuneResult)]
     L.pac_plan_destroy.argtypes = [_vp]
     L.pac_filter_spectrum.argtypes = [_vp, _vp, _vp, i, _vp, _vp, d, _vp]
     L.pac_convolve.argtypes = [_vp, _vp, _vp, _vp, _vp, i, _vp, _vp, d, _vp]
@@ -243,13 +251,63 @@ def dropin_twiddles(L, r, n):
 # ---------------------------------------------------------------------------
 # native plan API (device pointers)
 # ---------------------------------------------------------------------------
+class Tune(C.Structure):
+    """pac_tune_t: plan knobs (0 everywhere = the built-in choices)"""
+    _fields_ = [("max_factor_log", C.c_int), ("max_radix_log", C.c_int), ("special", C.c_int),
+                ("w_shift", C.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class TuneResult(C.Structure):
+    """pac_tune_result_t"""
+    _fields_ = [("tune", Tune), ("ms", C.c_double), ("default_ms", C.c_double),
+                ("candidates", C.c_int), ("cached", C.c_int)]
+
+
+def _tune(t):
+    if t is None or isinstance(t, Tune):
+        return t
+    return Tune(**t)
+
+
 class PlanInfo(C.Structure):
     """pac_plan_info_t"""
     _fields_ = [("n_elements", C.c_longlong), ("batch", C.c_longlong), ("rank", C.c_int),
                 ("dims", C.c_int * 3), ("digit_base", C.c_int), ("form", C.c_int),
                 ("element_bytes", C.c_int), ("conv_passes", C.c_int),
                 ("transform_passes", C.c_int), ("workspace_bytes", C.c_size_t),
-                ("digit_bases", C.c_int * 3)]
+                ("digit_bases", C.c_int * 3), ("tune", Tune)]
+
+
+def _bases(dims, digit_base):
+    if isinstance(digit_base, (tuple, list)):
+        return list(digit_base)
+    return [digit_base] * len(dims)
+
+
+def autotune(L, dims, batch=1, digit_base=2, form=PAC_FORM_F64, stream=None, cache=None):
+    """pac_autotune: the fastest knobs for one problem (read from `cache`, a
+    JSON-lines file, when it holds them; appended to it otherwise)."""
+    r = TuneResult()
+    arr = (C.c_int * len(dims))(*dims)
+    bases = (C.c_int * len(dims))(*_bases(dims, digit_base))
+    check(L, L.pac_autotune(len(dims), arr, bases, batch, form, stream,
+                            cache.encode() if cache else None, C.byref(r)), "pac_autotune")
+    return r
+
+
+def multi_autotune(L, shapes, digit_base=2, form=PAC_FORM_F32, stream=None, cache=None):
+    """pac_multi_autotune: one knob set for a whole uneven batch."""
+    r = TuneResult()
+    n = len(shapes)
+    ranks = (C.c_int * n)(*[len(s) for s in shapes])
+    dims = (C.c_int * (3 * n))(*[v for s in shapes for v in (tuple(s) + (1, 1, 1))[:3]])
+    check(L, L.pac_multi_autotune(n, ranks, dims, digit_base, form, stream,
+                                  cache.encode() if cache else None, C.byref(r)),
+          "pac_multi_autotune")
+    return r
 
 
 class MultiInfo(C.Structure):
@@ -262,14 +320,19 @@ class MultiPlan:
     """pac.h multi-plan: many convolutions of uneven shapes per call, over
     packed split arrays (problem p at elements offsets[p]:offsets[p+1])."""
 
-    def __init__(self, L, shapes, digit_base=2, form=PAC_FORM_F32):
+    def __init__(self, L, shapes, digit_base=2, form=PAC_FORM_F32, tune=None):
         self.L = L
         self.h = _vp()
         n = len(shapes)
         ranks = (C.c_int * n)(*[len(s) for s in shapes])
         dims = (C.c_int * (3 * n))(*[v for s in shapes for v in (tuple(s) + (1, 1, 1))[:3]])
-        check(L, L.pac_multi_create(C.byref(self.h), n, ranks, dims, digit_base, form),
-              "pac_multi_create")
+        t = _tune(tune)
+        if t is not None:
+            check(L, L.pac_multi_create_tuned(C.byref(self.h), n, ranks, dims, digit_base, form,
+                                              C.byref(t)), "pac_multi_create_tuned")
+        else:
+            check(L, L.pac_multi_create(C.byref(self.h), n, ranks, dims, digit_base, form),
+                  "pac_multi_create")
         off = (C.c_longlong * (n + 1))()
         check(L, L.pac_multi_offsets(self.h, off), "pac_multi_offsets")
         self.offsets = np.array(off[:], dtype=np.int64)
@@ -311,11 +374,16 @@ class MultiPlan:
 class Plan:
     """pac.h plan; device pointers are passed as integers."""
 
-    def __init__(self, L, dims, batch=1, digit_base=2, form=PAC_FORM_F64):
+    def __init__(self, L, dims, batch=1, digit_base=2, form=PAC_FORM_F64, tune=None):
         self.L = L
         self.h = _vp()
         arr = (C.c_int * len(dims))(*dims)
-        if isinstance(digit_base, (tuple, list)):  # one digit base per axis
+        t = _tune(tune)
+        if t is not None:  # explicit knobs (pac_tune_t)
+            bases = (C.c_int * len(dims))(*_bases(dims, digit_base))
+            check(L, L.pac_plan_create_tuned(C.byref(self.h), len(dims), arr, bases, batch, form,
+                                             C.byref(t)), "pac_plan_create_tuned")
+        elif isinstance(digit_base, (tuple, list)):  # one digit base per axis
             bases = (C.c_int * len(dims))(*digit_base)
             check(L, L.pac_plan_create_axes(C.byref(self.h), len(dims), arr, bases, batch, form),
                   "pac_plan_create_axes")
@@ -340,6 +408,11 @@ class Plan:
     def transform(self, op, in_re, in_im, out_re, out_im, stream=None):
         check(self.L, self.L.pac_transform(self.h, op, in_re, in_im, out_re, out_im, stream),
               "pac_transform")
+
+    def info(self):
+        inf = PlanInfo()
+        check(self.L, self.L.pac_plan_get_info(self.h, C.byref(inf)), "pac_plan_get_info")
+        return inf
 
     def close(self):
         if self.h:

@@ -16,6 +16,7 @@ enum { CPY_H2D = 0, CPY_D2H = 1, CPY_D2D = 2 };
 
 int be_init();  // PAC_SUCCESS when a usable device is present
 int be_num_sms();  // streaming multiprocessors of the current device (>= 1)
+int be_device_name(char* buf, int n);  // the current device's name (tuning cache key)
 int be_malloc(void** p, size_t bytes);
 int be_free(void* p);
 int be_memcpy(void* dst, const void* src, size_t bytes, int kind, void* stream);

@@ -470,6 +470,15 @@ int be_init() {
   return PAC_SUCCESS;
 }
 
+int be_device_name(char* buf, int n) {
+  int dev = 0;
+  PAC_CU(cudaGetDevice(&dev), "cudaGetDevice");
+  cudaDeviceProp prop;
+  PAC_CU(cudaGetDeviceProperties(&prop, dev), "cudaGetDeviceProperties");
+  snprintf(buf, (size_t)n, "%s", prop.name);
+  return PAC_SUCCESS;
+}
+
 int be_num_sms() {
   int dev = 0, n = 0;
   if (cudaGetDevice(&dev) != cudaSuccess ||

@@ -8,12 +8,14 @@
 // plan layer, the pass geometry and the kernels' index arithmetic can be
 // checked against the oracle on a machine without a GPU.
 #include <math.h>
+#include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
 #include <atomic>
 #include <limits>
+#include <chrono>
 #include <vector>
 
 #include "pac.h"
@@ -54,14 +56,29 @@ int be_stream_destroy(void*) { return PAC_SUCCESS; }
 int be_stream_sync(void*) { return PAC_SUCCESS; }
 int be_stream_wait(void*, void*) { return PAC_SUCCESS; }
 int be_l2_persist(void*, const void*, size_t) { return PAC_SUCCESS; }
+// events: host clock readings (the replay runs synchronously, so two
+// readings bracket the work issued between them)
 int be_event_create(void** ev) {
-  *ev = nullptr;
+  *ev = new double(0.0);
   return PAC_SUCCESS;
 }
-int be_event_destroy(void*) { return PAC_SUCCESS; }
-int be_event_record(void*, void*) { return PAC_SUCCESS; }
-int be_event_elapsed(void*, void*, float* ms) {
-  *ms = 0.f;
+int be_event_destroy(void* ev) {
+  delete (double*)ev;
+  return PAC_SUCCESS;
+}
+int be_event_record(void* ev, void*) {
+  if (ev)
+    *(double*)ev = std::chrono::duration<double, std::milli>(
+                       std::chrono::steady_clock::now().time_since_epoch())
+                       .count();
+  return PAC_SUCCESS;
+}
+int be_event_elapsed(void* a, void* b, float* ms) {
+  *ms = (a && b) ? (float)(*(double*)b - *(double*)a) : 0.f;
+  return PAC_SUCCESS;
+}
+int be_device_name(char* buf, int n) {
+  snprintf(buf, (size_t)n, "host replay");
   return PAC_SUCCESS;
 }
 

@@ -16,6 +16,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <string>
 #include <vector>
 
 #include "pac.h"
@@ -240,10 +241,10 @@ static int ilog_exact(int v, int b2) {
   return lg % b2 ? -1 : lg;
 }
 
-extern "C" {
-
-PAC_API int pac_multi_create(pac_multi_t* multi, int nprob, const int* ranks, const int* dims,
-                             int digit_base, int form) {
+// tune NULL: every shape's plan as pac_plan_create makes it (with the
+// knobs PAC_TUNE_CACHE holds for it, if any); else these knobs for all
+static int create_multi(pac_multi_t* multi, int nprob, const int* ranks, const int* dims,
+                        int digit_base, int form, const pac_tune_t* tune) {
   if (!multi || nprob < 1 || !ranks || !dims)
     return set_error(PAC_ERROR_INVALID_VALUE, "pac_multi_create: invalid arguments");
   if (digit_base == 0) digit_base = 2;
@@ -273,7 +274,9 @@ PAC_API int pac_multi_create(pac_multi_t* multi, int nprob, const int* ranks, co
     auto it = seen.find(key);
     if (it == seen.end()) {
       pac_plan_t pl = nullptr;
-      int st = pac_plan_create(&pl, r, key.data(), 1, digit_base, form);
+      const int bases[3] = {digit_base, digit_base, digit_base};
+      int st = tune ? pac_plan_create_tuned(&pl, r, key.data(), bases, 1, form, tune)
+                    : pac_plan_create(&pl, r, key.data(), 1, digit_base, form);
       if (st != PAC_SUCCESS) return st;
       it = seen.emplace(key, (int)m->plans.size()).first;
       m->plans.push_back(pl);
@@ -285,6 +288,30 @@ PAC_API int pac_multi_create(pac_multi_t* multi, int nprob, const int* ranks, co
   m->bytes = plan_bytes(m->plans[0]);
   *multi = m.release();
   return PAC_SUCCESS;
+}
+
+namespace pac {
+std::string plan_signature(pac_plan_s* pl);
+// every shape's plan schedule (pac_tune.cpp)
+std::string multi_signature(pac_multi_s* m) {
+  std::string sig;
+  for (auto* pl : m->plans) sig += plan_signature(pl) + "|";
+  return sig;
+}
+}  // namespace pac
+
+extern "C" {
+
+PAC_API int pac_multi_create(pac_multi_t* multi, int nprob, const int* ranks, const int* dims,
+                             int digit_base, int form) {
+  return create_multi(multi, nprob, ranks, dims, digit_base, form, nullptr);
+}
+
+PAC_API int pac_multi_create_tuned(pac_multi_t* multi, int nprob, const int* ranks,
+                                   const int* dims, int digit_base, int form,
+                                   const pac_tune_t* tune) {
+  static const pac_tune_t built_in = {0, 0, 0, 0};
+  return create_multi(multi, nprob, ranks, dims, digit_base, form, tune ? tune : &built_in);
 }
 
 PAC_API int pac_multi_destroy(pac_multi_t multi) {

@@ -31,6 +31,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <string>
 #include <vector>
 
 #include "pac.h"
@@ -73,6 +74,12 @@ struct Schedule {
   int bytes = 8;  // element bytes of one real component
   int b2 = 1;     // log2 of the digit base
   int tc = 0;     // tensor-core form: radix-16 stages on the tensor cores
+  // knobs (pac_tune_t): factor cap (0: built-in), largest stage radix (log2),
+  // specialised kernels (-1 off, 0 default, k > 0 k-th candidate), tile shift
+  int flog_cap = 0;
+  int rlog_cap = 4;
+  int special = 0;
+  int w_shift = 0;
   void* tcc = nullptr;  // its DFT operand table (tensor-core form)
   std::vector<VAx> vax;
   std::vector<std::vector<int>> rad;  // per factor: stage radix logs, DIF order
@@ -96,11 +103,20 @@ struct Schedule {
 
 static const int kSmemBudget = 200 * 1024;
 
-// stage radices of one factor of length 2^lg for digit base 2^b2 (the same
-// schedule the specialised kernels are compiled with, pac_special.h)
-static std::vector<int> radix_schedule(int lg, int b2) {
+// stage radices of one factor of length 2^lg for digit base 2^b2: with
+// stages of at most 4 bits the schedule the specialised kernels are compiled
+// with (sched_n / sched_v, pac_stages.cuh); a tuned plan may cap them at 3
+// bits (the same rule: fewest stages, bits spread evenly, larger first)
+static std::vector<int> radix_schedule(int lg, int b2, int rlog_cap = 4) {
   std::vector<int> r;
-  for (int i = 0; i < sched_n(lg, b2); ++i) r.push_back(sched_v(lg, b2, i));
+  if (rlog_cap >= 4 || b2 == 3) {
+    for (int i = 0; i < sched_n(lg, b2); ++i) r.push_back(sched_v(lg, b2, i));
+    return r;
+  }
+  const int per = rlog_cap / b2 > 0 ? rlog_cap / b2 : 1;  // digits per stage at most
+  const int digits = lg / b2;
+  const int n = (digits + per - 1) / per;
+  for (int i = 0; i < n; ++i) r.push_back((digits / n + (i < digits % n ? 1 : 0)) * b2);
   return r;
 }
 
@@ -108,10 +124,12 @@ static std::vector<int> radix_schedule(int lg, int b2) {
 // (64 KiB per line).  PAC_MAX_FACTOR_LOG lowers it, which forces more
 // factors per axis (used by the tests to reach 3- and 4-factor splits at
 // small sizes).
-static int max_factor_log(int bytes, int b2) {
+static int max_factor_log(int bytes, int b2, int cap = 0) {
   int lmax = bytes == 8 ? 12 : 13;
   const char* env = getenv("PAC_MAX_FACTOR_LOG");
-  if (env) {
+  if (cap > 0) {
+    if (cap >= b2 && cap < lmax) lmax = cap;
+  } else if (env) {
     int v = atoi(env);
     if (v >= b2 && v < lmax) lmax = v;
   }
@@ -125,7 +143,7 @@ static int build_schedule(Schedule& s, int rank, const int* logs, const int* b2s
     int lg = logs[a];
     if (lg == 0) continue;
     const int b2 = b2s[a];
-    const int lmax = max_factor_log(bytes, b2);
+    const int lmax = max_factor_log(bytes, b2, s.flog_cap);
     int digits = lg / b2;
     int dmax = lmax / b2;
     int nf = (digits + dmax - 1) / dmax;
@@ -141,7 +159,13 @@ static int build_schedule(Schedule& s, int rank, const int* logs, const int* b2s
     for (int f = 0; f < nf - 1; ++f) parts[f] = rest / (nf - 1) + (f < rest % (nf - 1) ? 1 : 0);
     for (int f = 0; f < nf; ++f) s.vax.push_back({parts[f] * b2, a, f == 0, f == nf - 1, b2});
   }
-  for (auto& v : s.vax) s.rad.push_back(radix_schedule(v.log, v.b2));
+  for (auto& v : s.vax) {
+    s.rad.push_back(radix_schedule(v.log, v.b2, s.rlog_cap));
+    if (s.rad.back().size() > (size_t)PAC_MAX_STAGES)
+      return set_error(PAC_ERROR_UNSUPPORTED_RADIX,
+                       "a factor of 2^%d needs %zu stages of radix <= 2^%d (at most %d)", v.log,
+                       s.rad.back().size(), s.rlog_cap, (int)PAC_MAX_STAGES);
+  }
   // stage twiddle tables
   std::vector<std::pair<int, int>> specs;
   long long total = 0;
@@ -198,6 +222,7 @@ struct pac_plan_s {
   int b2s[3] = {1, 1, 1};    // every axis's
   int form = PAC_FORM_F64;
   long long N = 1;
+  pac_tune_t tune = {0, 0, 0, 0};         // knobs the plan was built with
   pac::Schedule main;                     // storage type of the form
   std::unique_ptr<pac::Schedule> s64;     // FP64 schedule (F32 form: filter spectrum)
   std::mutex ws_mu;
@@ -250,6 +275,9 @@ static PassSpec make_pass(const Schedule& s, int vi, long long batch, long long 
     if (W < 16) W = 16;
     if (W > (1LL << logS)) W = 1LL << logS;
   }
+  if (s.w_shift > 0) W <<= s.w_shift;
+  if (s.w_shift < 0) W >>= -s.w_shift;
+  if (W < 1) W = 1;
   long long wmax = kSmemBudget / (2LL * esz * (base_pitch + NB));
   if (wmax < 1) wmax = 1;
   while (W > wmax) W >>= 1;
@@ -309,6 +337,9 @@ static void apply_special(const Schedule& s, PassSpec& p) {
   PassDesc& d = p.d;
   int logW = 0, nt = 0;
   if (d.nat) return;
+  // tuned off, or a radix schedule other than the one the specialised
+  // kernels are compiled with
+  if (s.special < 0 || s.rlog_cap < 4) return;
   // column pass whose tile a CTA cluster shares (W columns within the
   // stride, whole tiles), opt-in: PAC_CLUSTER_VARIANT=k picks the k-th
   // candidate geometry of the cluster list
@@ -352,7 +383,7 @@ static void apply_special(const Schedule& s, PassSpec& p) {
     return;
   }
   const char* var = getenv("PAC_SPECIAL_VARIANT");
-  const int variant = var ? atoi(var) : 0;
+  const int variant = s.special > 0 ? s.special : var ? atoi(var) : 0;
   const int cols = d.logS > 0 ? 1 : 0;
   if (!special_geometry(s.bytes, p.b2, d.mode, d.sign, d.logL, cols, d.tc, &logW, &nt, variant) &&
       !special_geometry(s.bytes, p.b2, d.mode, d.sign, d.logL, cols, d.tc, &logW, &nt))
@@ -580,6 +611,17 @@ int plan_conv_descs(pac_plan_s* pl, const void* x_re, const void* x_im, const vo
   return PAC_SUCCESS;
 }
 int plan_bytes(pac_plan_s* pl) { return pl->main.bytes; }
+// the factor lengths and stage radices of the plan (the autotuner skips a
+// knob set whose schedule it has already timed)
+std::string plan_signature(pac_plan_s* pl) {
+  std::string sig;
+  for (size_t i = 0; i < pl->main.vax.size(); ++i) {
+    sig += std::to_string(pl->main.vax[i].log) + ":";
+    for (int r : pl->main.rad[i]) sig += std::to_string(r) + ",";
+    sig += ";";
+  }
+  return sig;
+}
 int plan_b2(pac_plan_s* pl) { return pl->b2; }
 
 // P-order FP64 spectrum -> the plan's spectrum storage: every block of R
@@ -717,12 +759,25 @@ static int ilog2_exact(long long v, int b2) {
   return lg;
 }
 
+namespace pac {
+// pac_tune.cpp: the knobs PAC_TUNE_CACHE holds for this device and problem
+bool tune_from_env_cache(int rank, const int* dims, const int* bases, int batch, int form,
+                         pac_tune_t* tune);
+}  // namespace pac
+
 extern "C" {
 
-PAC_API int pac_plan_create_axes(pac_plan_t* plan, int rank, const int* dims,
-                                 const int* digit_bases, int batch, int form) {
+static int create_plan(pac_plan_t* plan, int rank, const int* dims, const int* digit_bases,
+                       int batch, int form, const pac_tune_t* tune) {
   if (!plan || !dims || !digit_bases || rank < 1 || rank > 3 || batch < 1)
     return set_error(PAC_ERROR_INVALID_VALUE, "pac_plan_create: invalid rank/dims/batch");
+  const pac_tune_t knobs = tune ? *tune : pac_tune_t{0, 0, 0, 0};
+  if (knobs.max_factor_log < 0 || knobs.max_factor_log > 13 || knobs.max_radix_log < 0 ||
+      knobs.max_radix_log > 4 || knobs.special < -1 || knobs.w_shift < -6 || knobs.w_shift > 6)
+    return set_error(PAC_ERROR_INVALID_VALUE,
+                     "pac_plan_create: knobs out of range (factor log %d, radix log %d, "
+                     "special %d, w shift %d)",
+                     knobs.max_factor_log, knobs.max_radix_log, knobs.special, knobs.w_shift);
   int b2s[3] = {1, 1, 1};
   for (int a = 0; a < rank; ++a) {
     const int base = digit_bases[a] == 0 ? 2 : digit_bases[a];
@@ -754,6 +809,11 @@ PAC_API int pac_plan_create_axes(pac_plan_t* plan, int rank, const int* dims,
   if (N * (long long)batch > (1LL << 40) || N > (1LL << 31))
     return set_error(PAC_ERROR_SIZE, "pac_plan_create: problem too large");
   p->N = N;
+  p->tune = knobs;
+  p->main.flog_cap = knobs.max_factor_log;
+  p->main.rlog_cap = knobs.max_radix_log > 0 ? knobs.max_radix_log : 4;
+  p->main.special = knobs.special;
+  p->main.w_shift = knobs.w_shift;
   int bytes = form == PAC_FORM_F64 ? 8 : 4;
   st = build_schedule(p->main, rank, p->logs, b2s, bytes);
   if (st != PAC_SUCCESS) return st;
@@ -770,6 +830,21 @@ PAC_API int pac_plan_create_axes(pac_plan_t* plan, int rank, const int* dims,
   }
   *plan = p.release();
   return PAC_SUCCESS;
+}
+
+PAC_API int pac_plan_create_tuned(pac_plan_t* plan, int rank, const int* dims,
+                                  const int* digit_bases, int batch, int form,
+                                  const pac_tune_t* tune) {
+  return create_plan(plan, rank, dims, digit_bases, batch, form, tune);
+}
+
+PAC_API int pac_plan_create_axes(pac_plan_t* plan, int rank, const int* dims,
+                                 const int* digit_bases, int batch, int form) {
+  pac_tune_t t;
+  if (dims && digit_bases && rank >= 1 && rank <= 3 &&
+      tune_from_env_cache(rank, dims, digit_bases, batch, form, &t))
+    return create_plan(plan, rank, dims, digit_bases, batch, form, &t);
+  return create_plan(plan, rank, dims, digit_bases, batch, form, nullptr);
 }
 
 PAC_API int pac_plan_create(pac_plan_t* plan, int rank, const int* dims, int batch,
@@ -798,6 +873,7 @@ PAC_API int pac_plan_get_info(pac_plan_t plan, pac_plan_info_t* info) {
   info->conv_passes = m == 0 ? 1 : 2 * m - 1;
   info->transform_passes = m == 0 ? 1 : m;
   info->workspace_bytes = plan->ws_bytes + plan->tmp64_bytes;
+  info->tune = plan->tune;
   return PAC_SUCCESS;
 }
 

@@ -77,6 +77,24 @@ enum {
   PAC_OP_UIFFT = 6    /* conj(A) x / N             uifft                           */
 };
 
+/* Plan knobs the autotuner chooses (0 everywhere = the built-in choices,
+ * which the environment variables PAC_MAX_FACTOR_LOG and
+ * PAC_SPECIAL_VARIANT may still adjust):
+ *   max_factor_log  longest axis factor one CTA transforms, log2 (lower
+ *                   values split an axis into more, shorter factors)
+ *   max_radix_log   largest stage radix, log2: 4 (radix 16) or 3 (radix 8)
+ *   special         -1: every pass on the generic kernel; 0: the specialised
+ *                   kernel of the pass's geometry where one exists; k > 0:
+ *                   its k-th candidate
+ *   w_shift         lines per CTA of generic passes times 2^w_shift
+ * No counterpart in the reference, which has one fixed schedule per radix. */
+typedef struct {
+  int max_factor_log;
+  int max_radix_log;
+  int special;
+  int w_shift;
+} pac_tune_t;
+
 typedef struct {
   long long n_elements;   /* elements of one problem (product of dims)    */
   long long batch;
@@ -89,6 +107,7 @@ typedef struct {
   int transform_passes;   /* kernel launches of one forward transform     */
   size_t workspace_bytes; /* device workspace held by the plan            */
   int digit_bases[3];     /* per axis (digit_base is axis 0's)            */
+  pac_tune_t tune;        /* the knobs the plan was built with            */
 } pac_plan_info_t;
 
 /* Plan for `batch` problems of shape dims[0..rank-1] (rank 1..3).  Every
@@ -106,6 +125,33 @@ PAC_API int pac_plan_create(pac_plan_t* plan, int rank, const int* dims, int bat
  * it runs at bases 8, 4 and 2. */
 PAC_API int pac_plan_create_axes(pac_plan_t* plan, int rank, const int* dims,
                                  const int* digit_bases, int batch, int form);
+/* As pac_plan_create_axes with explicit knobs (tune NULL: the built-in
+ * choices).  pac_plan_create and pac_plan_create_axes use the knobs cached
+ * for the problem in the file named by the environment variable
+ * PAC_TUNE_CACHE, when it names one and holds an entry for this device and
+ * problem (pac_autotune writes them). */
+PAC_API int pac_plan_create_tuned(pac_plan_t* plan, int rank, const int* dims,
+                                  const int* digit_bases, int batch, int form,
+                                  const pac_tune_t* tune);
+
+/* Autotuner: times candidate knob sets for one problem on the current
+ * device (convolutions of device buffers it allocates and frees itself,
+ * issued on `stream`, which it synchronises) -- a coordinate descent over
+ * the kernel choice, the largest stage radix, the factor length and the
+ * tile width, each step kept only if it is at least 2% faster -- and
+ * returns the fastest.  With cache_path non-NULL it first looks the
+ * problem up there and, when it tuned, appends the result as one JSON line
+ * ({"key": ..., "max_factor_log": ..., ..., "ms": ..., "default_ms": ...}).
+ * No counterpart in the reference. */
+typedef struct {
+  pac_tune_t tune;     /* the fastest knobs                               */
+  double ms;           /* its time per convolution                        */
+  double default_ms;   /* the built-in knobs' time                        */
+  int candidates;      /* knob sets timed (0 when read from the cache)    */
+  int cached;          /* 1: read from cache_path, nothing was timed      */
+} pac_tune_result_t;
+PAC_API int pac_autotune(int rank, const int* dims, const int* digit_bases, int batch, int form,
+                         pac_stream_t stream, const char* cache_path, pac_tune_result_t* result);
 /* free_twiddles (twiddle_factors.c:133) */
 PAC_API int pac_plan_destroy(pac_plan_t plan);
 PAC_API int pac_plan_get_info(pac_plan_t plan, pac_plan_info_t* info);
@@ -217,6 +263,17 @@ typedef struct {
   long long timed_calls;  /* calls behind level_ms */
 } pac_multi_info_t;
 PAC_API int pac_multi_get_info(pac_multi_t multi, pac_multi_info_t* info);
+/* As pac_multi_create with one set of knobs for every shape's plan. */
+PAC_API int pac_multi_create_tuned(pac_multi_t* multi, int nprob, const int* ranks,
+                                   const int* dims, int digit_base, int form,
+                                   const pac_tune_t* tune);
+/* pac_autotune for a whole uneven batch: the knob set under which one
+ * pac_multi_convolve of all the problems is fastest (the work-queue kernel
+ * is generic, so `special` is not searched); cached under a key that lists
+ * every problem's shape. */
+PAC_API int pac_multi_autotune(int nprob, const int* ranks, const int* dims, int digit_base,
+                               int form, pac_stream_t stream, const char* cache_path,
+                               pac_tune_result_t* result);
 /* Level timing: while enabled, pac_multi_convolve issues the levels
  * directly (no graph), records a CUDA event around every level on the
  * caller's stream and waits for them (calls become synchronous);

@@ -90,12 +90,12 @@ class Dev:
         self.ptrs = []
 
 
-def native_conv(L, dims, batch, base, form, x, h, per_problem=False):
+def native_conv(L, dims, batch, base, form, x, h, per_problem=False, tune=None):
     """pac_filter_spectrum + pac_convolve on host arrays; returns y (complex)."""
     dt = np.float64 if form == pac.PAC_FORM_F64 else np.float32
     d = Dev(L)
     try:
-        plan = pac.Plan(L, dims, batch, base, form)
+        plan = pac.Plan(L, dims, batch, base, form, tune=tune)
         nf = batch if per_problem else 1
         hshape = (nf,) + tuple(dims)
         hr = d.put(np.real(h).reshape(hshape).astype(np.float64))
@@ -211,14 +211,14 @@ def check_column_kernels(L, orc, dims, batch, form, monkeypatch, kind):
             assert crel(t[b], zr + 1j * zi) < TOL
 
 
-def check_multi(L, shapes, form, stream=False, seed=3):
+def check_multi(L, shapes, form, stream=False, seed=3, tune=None):
     """pac_multi_*: every problem of an uneven batch against numpy's FP64
     FFT convolution; a second call (the CUDA-graph replay when a stream is
     given) repeats the first bit for bit."""
     dt = np.float64 if form == pac.PAC_FORM_F64 else np.float32
     tol = TOL if form == pac.PAC_FORM_F64 else TOL_TC if form == pac.PAC_FORM_TC else TOL_F32
     g = rng(seed)
-    m = pac.MultiPlan(L, shapes, 2, form)
+    m = pac.MultiPlan(L, shapes, 2, form, tune=tune)
     off = m.offsets
     n = int(off[-1])
     xs, hs = [], []
@@ -343,3 +343,63 @@ def check_tc(L, orc, dims, batch, base, seed=5, ops=True):
     for k, (l2, mx) in errs.items():
         assert l2 < TOL_TC, (dims, base, k, l2, mx)
     return errs
+
+
+# knob sets of the autotuner's search (pac_tune_t), each of which must give
+# the same convolution as the built-in knobs
+TUNE_CANDIDATES = [
+    {"max_factor_log": 0, "max_radix_log": 0, "special": -1, "w_shift": 0},
+    {"max_factor_log": 0, "max_radix_log": 3, "special": 0, "w_shift": 0},
+    {"max_factor_log": 8, "max_radix_log": 0, "special": 0, "w_shift": 0},
+    {"max_factor_log": 6, "max_radix_log": 3, "special": 0, "w_shift": 1},
+    {"max_factor_log": 0, "max_radix_log": 0, "special": 0, "w_shift": -1},
+    {"max_factor_log": 0, "max_radix_log": 2, "special": 0, "w_shift": 2},
+]
+
+
+def check_tuned(L, dims, batch, base, form, tune, seed=6):
+    """A tuned plan's convolution against numpy's FP64 FFT convolution; the
+    plan reports the knobs it was built with."""
+    g = rng(seed)
+    shape = (batch,) + tuple(dims)
+    x = g.standard_normal(shape) + 1j * g.standard_normal(shape)
+    h = g.standard_normal(dims) + 1j * g.standard_normal(dims)
+    y = native_conv(L, dims, batch, base, form, x, h, tune=tune)
+    z = fftconv(x, h[None], tuple(range(1, len(shape))))
+    tol = {pac.PAC_FORM_F64: TOL, pac.PAC_FORM_F32: TOL_F32, pac.PAC_FORM_TC: TOL_TC}[form]
+    assert crel(y, z) < tol, (dims, tune, crel(y, z))
+    plan = pac.Plan(L, dims, batch, base, form, tune=tune)
+    got = plan.info().tune.as_dict()
+    plan.close()
+    assert got == tune
+    return crel(y, z)
+
+
+def check_autotune(L, cache, dims, batch, base, form):
+    """pac_autotune: a result, appended to the cache as one JSON line and read
+    back on the second call without timing; plans made by pac_plan_create
+    with PAC_TUNE_CACHE set carry the cached knobs and convolve correctly."""
+    import json
+    import os
+    r1 = pac.autotune(L, dims, batch, base, form, cache=cache)
+    assert r1.cached == 0 and r1.candidates >= 3 and r1.ms > 0 and r1.default_ms > 0
+    assert r1.ms <= r1.default_ms
+    lines = [json.loads(s) for s in open(cache).read().splitlines()]
+    assert lines[-1]["max_radix_log"] == r1.tune.max_radix_log
+    assert lines[-1]["candidates"] == r1.candidates
+    r2 = pac.autotune(L, dims, batch, base, form, cache=cache)
+    assert r2.cached == 1 and r2.candidates == 0
+    assert r2.tune.as_dict() == r1.tune.as_dict()
+    old = os.environ.get("PAC_TUNE_CACHE")
+    os.environ["PAC_TUNE_CACHE"] = cache
+    try:
+        plan = pac.Plan(L, dims, batch, base, form)
+        assert plan.info().tune.as_dict() == r1.tune.as_dict()
+        plan.close()
+        check_tuned(L, dims, batch, base, form, r1.tune.as_dict())
+    finally:
+        if old is None:
+            del os.environ["PAC_TUNE_CACHE"]
+        else:
+            os.environ["PAC_TUNE_CACHE"] = old
+    return r1

@@ -227,3 +227,80 @@ def test_tc_form_split_axes(emu, orc, monkeypatch):
 def test_tc_multi(emu):
     shapes = [(256,), (2048, 16), (16, 16, 16), (4096,), (2,)]
     P.check_multi(emu, shapes, pac.PAC_FORM_TC)
+
+
+# Autotuner knobs (pac_tune_t): every knob set of the search builds a plan
+# whose convolution is the built-in plan's (factor splits, radix-8 and
+# radix-4 schedules, generic kernels only, other tile widths), and the
+# tuner itself over the replay backend (whose events read the host clock).
+@pytest.mark.parametrize("tune", P.TUNE_CANDIDATES)
+@pytest.mark.parametrize("dims,batch,base,form", [
+    ((4096,), 2, 2, 0), ((64, 2048), 1, 2, 1), ((2048, 32), 1, 2, 2), ((4096,), 1, 4, 1),
+    ((16, 32, 64), 2, 2, 0)])
+def test_tuned_plans(emu, dims, batch, base, form, tune):
+    P.check_tuned(emu, dims, batch, base, form, tune)
+
+
+def test_tune_knob_errors(emu):
+    with pytest.raises(pac.PacError):
+        pac.Plan(emu, (64,), 1, 2, 0, tune={"max_factor_log": 0, "max_radix_log": 5,
+                                            "special": 0, "w_shift": 0})
+    with pytest.raises(pac.PacError):
+        pac.Plan(emu, (64,), 1, 2, 0, tune={"max_factor_log": 0, "max_radix_log": 0,
+                                            "special": -2, "w_shift": 0})
+    # radix-2 stages of a 2^12 factor: more stages than a pass holds
+    with pytest.raises(pac.PacError):
+        pac.Plan(emu, (4096,), 1, 2, 0, tune={"max_factor_log": 0, "max_radix_log": 1,
+                                              "special": 0, "w_shift": 0})
+    plan = pac.Plan(emu, (256,), 1, 2, 0, tune={"max_factor_log": 0, "max_radix_log": 1,
+                                                "special": 0, "w_shift": 0})
+    plan.close()
+
+
+def test_autotune_cache(emu, tmp_path):
+    P.check_autotune(emu, str(tmp_path / "tune.jsonl"), (1024,), 2, 2, 1)
+
+
+def test_multi_autotune(emu, tmp_path):
+    shapes = [(256,), (64, 32), (1024,), (16, 16, 16)]
+    cache = str(tmp_path / "tune.jsonl")
+    r = pac.multi_autotune(emu, shapes, 2, 1, cache=cache)
+    assert r.cached == 0 and r.candidates >= 2 and r.tune.special == 0
+    r2 = pac.multi_autotune(emu, shapes, 2, 1, cache=cache)
+    assert r2.cached == 1 and r2.tune.as_dict() == r.tune.as_dict()
+    for t in (r.tune.as_dict(), P.TUNE_CANDIDATES[3]):
+        P.check_multi(emu, shapes, 1, tune=t)
+
+
+def test_tune_knobs_take_effect(emu):
+    """The factor cap changes the pass count; the radix cap changes the last
+    stage radix of the innermost factor, which is the block size of the
+    filter spectrum's plan order (pac_filter_spectrum output) -- while the
+    convolutions agree (test_tuned_plans)."""
+    def knobs(**kw):
+        t = {"max_factor_log": 0, "max_radix_log": 0, "special": 0, "w_shift": 0}
+        t.update(kw)
+        return t
+    passes = {}
+    for cap in (0, 8, 6, 4):
+        plan = pac.Plan(emu, (4096,), 1, 2, 0, tune=knobs(max_factor_log=cap))
+        passes[cap] = plan.info().conv_passes
+        plan.close()
+    assert passes == {0: 1, 8: 3, 6: 3, 4: 5}
+    g = rng(3)
+    h = g.standard_normal(4096) + 1j * g.standard_normal(4096)
+    d = P.Dev(emu)
+    try:
+        hr, hi = d.put(h.real.copy()), d.put(h.imag.copy())
+        outs = []
+        for rl in (0, 3):
+            plan = pac.Plan(emu, (4096,), 1, 2, 0, tune=knobs(max_radix_log=rl))
+            Hr, Hi = d.zeros(4096, np.float64), d.zeros(4096, np.float64)
+            plan.filter_spectrum(hr, hi, Hr, Hi)
+            outs.append(d.get(Hr, 4096, np.float64) + 1j * d.get(Hi, 4096, np.float64))
+            plan.close()
+    finally:
+        d.free()
+    # same values (the P-order spectrum), different plan orders
+    assert not np.allclose(outs[0], outs[1])
+    assert np.allclose(np.sort_complex(outs[0]), np.sort_complex(outs[1]), atol=1e-12)

@@ -296,3 +296,30 @@ def test_c4_3d_tc(lib, shape):
     y = P.native_conv(lib, shape, 1, 2, pac.PAC_FORM_TC, x, h)[0]
     z = P.fftconv(x, h, (0, 1, 2))
     assert P.crel(y, z) < P.TOL_TC
+
+
+# Autotuner: every knob set of its search gives the built-in plan's
+# convolution on the device (specialised kernels off, radix-8 / radix-4
+# schedules, other factor splits and tile widths), and the tuner's cache
+# round trip on the device's own timings.
+@pytest.mark.parametrize("tune", P.TUNE_CANDIDATES)
+@pytest.mark.parametrize("dims,batch,base,form", [
+    ((2048, 2048), 1, 2, 1), ((65536,), 4, 2, 0), ((256, 256, 256), 1, 2, 1),
+    ((64, 2048), 2, 2, 2), ((4096,), 3, 4, 0)])
+def test_tuned_plans(lib, dims, batch, base, form, tune):
+    P.check_tuned(lib, dims, batch, base, form, tune)
+
+
+@pytest.mark.parametrize("dims,batch,base,form", [((2048, 2048), 1, 2, 1), ((65536,), 64, 2, 0)])
+def test_autotune_cache(lib, tmp_path, dims, batch, base, form):
+    P.check_autotune(lib, str(tmp_path / "tune.jsonl"), dims, batch, base, form)
+
+
+def test_multi_autotune(lib, tmp_path):
+    shapes = [(256,), (2048, 64), (4096,), (16, 16, 16), (65536,), (512, 512)]
+    cache = str(tmp_path / "tune.jsonl")
+    r = pac.multi_autotune(lib, shapes, 2, 1, cache=cache)
+    assert r.cached == 0 and r.candidates >= 2 and r.ms <= r.default_ms
+    r2 = pac.multi_autotune(lib, shapes, 2, 1, cache=cache)
+    assert r2.cached == 1 and r2.tune.as_dict() == r.tune.as_dict()
+    P.check_multi(lib, shapes, 1, stream=True, tune=r.tune.as_dict())
