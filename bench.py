@@ -283,10 +283,11 @@ def run_ours(args, world, dist):
     y = (ybuf[0], ybuf[1])
     stream = torch.cuda.current_stream(dev)
     sp = stream.cuda_stream
+    # tuning first, with no L2 window set: every candidate is timed alike
+    tuned = tune_workload(L, args, dims, batch, form, sp)
     l2_bytes = ybuf.numel() * ybuf.element_size() if args.l2 == "on" else 0
     if l2_bytes:
         pac.check(L, L.pac_stream_set_l2_persisting(sp, ybuf.data_ptr(), l2_bytes), "l2")
-    tuned = tune_workload(L, args, dims, batch, form, sp)
     plan = pac.Plan(L, dims, batch, 2, form)  # the tuned knobs, through PAC_TUNE_CACHE
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
