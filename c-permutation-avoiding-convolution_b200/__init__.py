@@ -313,7 +313,8 @@ def multi_autotune(L, shapes, digit_base=2, form=PAC_FORM_F32, stream=None, cach
 class MultiInfo(C.Structure):
     _fields_ = [("nprob", C.c_int), ("nshapes", C.c_int), ("nlevels", C.c_int),
                 ("items", C.c_longlong * 8), ("elements", C.c_longlong), ("graph", C.c_int),
-                ("level_ms", C.c_double * 8), ("timed_calls", C.c_longlong)]
+                ("level_ms", C.c_double * 8), ("timed_calls", C.c_longlong),
+                ("fast_items", C.c_longlong)]
 
 
 class MultiPlan:
@@ -353,7 +354,7 @@ class MultiPlan:
         return {"nprob": inf.nprob, "nshapes": inf.nshapes, "nlevels": inf.nlevels,
                 "items": list(inf.items[:inf.nlevels]), "elements": inf.elements,
                 "graph": inf.graph, "level_ms": list(inf.level_ms[:inf.nlevels]),
-                "timed_calls": inf.timed_calls}
+                "timed_calls": inf.timed_calls, "fast_items": inf.fast_items}
 
     def set_level_timing(self, enable):
         check(self.L, self.L.pac_multi_set_level_timing(self.h, 1 if enable else 0),

@@ -136,7 +136,7 @@ __global__ void __launch_bounds__(256) pac_queue_kernel(const PassDesc* __restri
       s_lb[64 + threadIdx.x] = s_lb[threadIdx.x];
     }
     __syncthreads();
-    pass_body<T, B2, TC>(sd, cta, sre, sim, s_lb, s_lb + 64);
+    queue_pass_body<T, B2, TC>(sd, cta, sre, sim, s_lb, s_lb + 64);
     __syncthreads();  // sd, s_lb and the tile are reused by the next item
   }
 }

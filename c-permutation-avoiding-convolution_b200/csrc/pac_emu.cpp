@@ -422,8 +422,8 @@ static void replay_queue(const PassDesc* descs, const long long* starts, const i
     const long long cta = it - starts[k];
     std::vector<T> sm((size_t)2 * d.W * d.pitch, std::numeric_limits<T>::quiet_NaN());
     for (int w = 0; w < d.W; ++w) lb[w] = lb[64 + w] = line_base(d, cta * d.W + w);
-    pass_body<T, B2, TC>(d, cta, sm.data(), sm.data() + (size_t)d.W * d.pitch, lb.data(),
-                         lb.data() + 64);
+    queue_pass_body<T, B2, TC>(d, cta, sm.data(), sm.data() + (size_t)d.W * d.pitch, lb.data(),
+                               lb.data() + 64);
   }
 }
 

@@ -82,6 +82,7 @@ struct pac_multi_s {
   std::vector<void*> ev;
   double level_ms[kMaxLevels] = {};
   long long timed_calls = 0;
+  long long fast_items = 0;  // work items of descriptors marked special
   ~pac_multi_s() {
     for (void* e : ev) be_event_destroy(e);
     if (graph) be_graph_destroy(graph);
@@ -126,6 +127,7 @@ static int build_levels(pac_multi_s* m, const void* x_re, const void* x_im, cons
     }
   }
   m->levels.assign(nlev, {});
+  long long fast = 0;
   size_t bytes = 0;
   for (size_t k = 0; k < nlev; ++k)
     for (int g = 0; g < kGroups; ++g) {
@@ -138,6 +140,7 @@ static int build_levels(pac_multi_s* m, const void* x_re, const void* x_im, cons
       for (auto& it : items) {
         G.total += it.ctas;
         G.smem = std::max(G.smem, it.smem);
+        if (it.d.spec) fast += it.ctas;
       }
       G.desc_off = bytes;
       bytes += round256(sizeof(PassDesc) * G.ndesc);
@@ -147,6 +150,7 @@ static int build_levels(pac_multi_s* m, const void* x_re, const void* x_im, cons
       bytes += round256(sizeof(int) * (size_t)G.total);
       m->levels[k].push_back(G);
     }
+  m->fast_items = fast;
   m->counter_off = bytes;
   bytes += round256(sizeof(unsigned long long) * kMaxLevels * kGroups);
   std::vector<unsigned char> host(bytes, 0);
@@ -389,6 +393,7 @@ PAC_API int pac_multi_get_info(pac_multi_t m, pac_multi_info_t* info) {
   info->elements = m->off[m->nprob];
   info->graph = m->graph ? 1 : 0;
   info->timed_calls = m->timed_calls;
+  info->fast_items = m->fast_items;
   for (size_t k = 0; k < m->levels.size() && k < kMaxLevels; ++k)
     info->level_ms[k] = m->timed_calls ? m->level_ms[k] / (double)m->timed_calls : 0.0;
   return PAC_SUCCESS;

@@ -401,6 +401,27 @@ static void apply_special(const Schedule& s, PassSpec& p) {
   p.smem = (size_t)2 * d.W * d.pitch * s.bytes;
 }
 
+// A multi-plan pass whose geometry has a work-queue fast path
+// (PAC_QUEUE_LIST): its tile width, and the mark that selects the
+// compile-time body inside pac_queue_kernel.
+static void apply_queue_special(const Schedule& s, PassSpec& p) {
+  PassDesc& d = p.d;
+  int logW = 0;
+  const int cols = d.logS > 0 ? 1 : 0;
+  if (d.nat || s.special < 0 || s.rlog_cap < 4) return;
+  if (!queue_geometry(s.bytes, p.b2, d.mode, d.sign, d.logL, cols, d.tc, &logW)) return;
+  const long long W = 1LL << logW;
+  if ((d.nlines & (W - 1)) != 0 || (cols && logW > d.logS)) return;
+  d.W = (int)W;
+  d.logW = logW;
+  d.pitch = pitch_for(s.bytes, d.logL, d.W, cols, d.tc);
+  d.nthreads = PAC_QUEUE_THREADS;
+  d.spec = 1;
+  p.threads = PAC_QUEUE_THREADS;
+  p.grid = d.nlines / W;
+  p.smem = (size_t)2 * d.W * d.pitch * s.bytes;
+}
+
 static int launch(const Schedule& s, PassSpec& p, void* stream) {
   return be_launch_pass(p.d, s.bytes, p.b2, p.grid, p.threads, p.smem, stream);
 }
@@ -603,6 +624,7 @@ int plan_conv_descs(pac_plan_s* pl, const void* x_re, const void* x_im, const vo
   std::vector<PassSpec> passes;
   if (!pl->main.vax.empty())
     build_conv_passes(pl, x_re, x_im, h_re, h_im, 0, y_re, y_im, 1.0, passes);
+  for (auto& p : passes) apply_queue_special(pl->main, p);
   for (auto& p : passes) {
     descs.push_back(p.d);
     ctas.push_back(p.grid);

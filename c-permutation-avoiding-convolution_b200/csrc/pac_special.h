@@ -90,6 +90,60 @@ namespace pac {
   X(float, 4, 1, MODE_DIF, -1, 11, 3, 512)          \
   X(float, 4, 1, MODE_DIT, +1, 11, 3, 512)
 
+// Work-queue fast paths (pac_queue_kernel, 256 threads): multi-plan passes
+// of these geometries get their tile width and run the compile-time body
+// (pass_body_ct) inside the persistent queue kernel; all others run the
+// generic body.  The FP32 base-2 geometries that carry most of the elements
+// of uneven 1D/2D batches (fused 2048-point rows; 512-, 256- and 128-point
+// columns, the outer factors of 2^18..2^20-point lines).
+// fields: element type, bytes, log2 digit base, mode, sign, log2 L, column
+// tile, log2 W, tensor-core form
+#define PAC_QUEUE_LIST(X)                            \
+  X(float, 4, 1, MODE_CONV, 0, 11, 0, 1, 0)          \
+  X(float, 4, 1, MODE_DIF, -1, 9, 1, 4, 0)           \
+  X(float, 4, 1, MODE_DIT, +1, 9, 1, 4, 0)           \
+  X(float, 4, 1, MODE_DIF, -1, 8, 1, 4, 0)           \
+  X(float, 4, 1, MODE_DIT, +1, 8, 1, 4, 0)           \
+  X(float, 4, 1, MODE_DIF, -1, 7, 1, 5, 0)           \
+  X(float, 4, 1, MODE_DIT, +1, 7, 1, 5, 0)
+enum { PAC_QUEUE_THREADS = 256 };
+
+inline bool queue_geometry(int bytes, int b2, int mode, int sign, int logL, int cols, int tc,
+                           int* logW) {
+#define PAC_X(T, BY, B2_, MO, SG, LL, CO, LW, TC_)                                     \
+  if (bytes == BY && b2 == B2_ && mode == MO && (MO == MODE_CONV || sign == SG) &&  \
+      logL == LL && cols == CO && tc == TC_) {                                      \
+    *logW = LW;                                                                     \
+    return true;                                                                    \
+  }
+  PAC_QUEUE_LIST(PAC_X)
+#undef PAC_X
+  return false;
+}
+
+// One work item of the queue kernel (device) or of its host replay: the
+// compile-time body when the descriptor is marked special and its geometry
+// is on PAC_QUEUE_LIST, else the generic body.
+template <typename T, int B2, int TC>
+PAC_HD void queue_pass_body(const PassDesc& d, long long cta, T* sre, T* sim, const long long* lbi,
+                            const long long* lbo) {
+  if (d.spec) {
+#define PAC_X(T_, BY, B2_, MO, SG, LL, CO, LW, TC_)                                          \
+    if constexpr (sizeof(T) == BY && B2 == B2_ && TC == TC_) {                            \
+      if (d.mode == MO && (MO == MODE_CONV || d.sign == SG) && d.logL == LL &&            \
+          (d.logS > 0 ? 1 : 0) == CO && d.logW == LW) {                                   \
+        constexpr int P_ = pitch_for(BY, LL, 1 << LW, CO, TC_);                           \
+        pass_body_ct<T, B2, MO, SG, Shape<LL, LW, P_, CO, TC_>, PAC_QUEUE_THREADS,        \
+                     RadsFor<LL, B2>, TC_>(d, cta, sre, sim, lbi, lbo);                   \
+        return;                                                                           \
+      }                                                                                   \
+    }
+    PAC_QUEUE_LIST(PAC_X)
+#undef PAC_X
+  }
+  pass_body<T, B2, TC>(d, cta, sre, sim, lbi, lbo);
+}
+
 inline bool pipe_geometry(int bytes, int b2, int mode, int sign, int logL, int* logW, int* nt) {
 #define PAC_X(T, BY, B2_, MO, SG, LL, LW, NT_)                                      \
   if (bytes == BY && b2 == B2_ && mode == MO && sign == SG && logL == LL) {      \

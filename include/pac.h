@@ -261,6 +261,7 @@ typedef struct {
   int graph;              /* 1 once a CUDA graph replays the levels */
   double level_ms[8];     /* per-level mean time of the timed calls */
   long long timed_calls;  /* calls behind level_ms */
+  long long fast_items;   /* work items on compile-time bodies (work-queue fast paths) */
 } pac_multi_info_t;
 PAC_API int pac_multi_get_info(pac_multi_t multi, pac_multi_info_t* info);
 /* As pac_multi_create with one set of knobs for every shape's plan. */

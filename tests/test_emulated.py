@@ -304,3 +304,19 @@ def test_tune_knobs_take_effect(emu):
     # same values (the P-order spectrum), different plan orders
     assert not np.allclose(outs[0], outs[1])
     assert np.allclose(np.sort_complex(outs[0]), np.sort_complex(outs[1]), atol=1e-12)
+
+
+
+# Work-queue fast paths (PAC_QUEUE_LIST): with factors of at most 2^11 these
+# shapes put fused 2048-point rows and 512-, 256- and 128-point columns on
+# the compile-time bodies inside the queue kernel.
+QUEUE_FAST_SHAPES = [(2 ** 18,), (256, 2048), (512, 64), (2048,), (128, 2048), (2 ** 17,), (64, 32)]
+CAP11 = {"max_factor_log": 11, "max_radix_log": 0, "special": 0, "w_shift": 0}
+
+
+def test_multi_queue_fast_paths(emu):
+    info = P.check_multi(emu, QUEUE_FAST_SHAPES, 1, tune=CAP11)
+    assert 0 < info["fast_items"] < sum(info["items"])
+    off = dict(CAP11, special=-1)
+    info = P.check_multi(emu, QUEUE_FAST_SHAPES, 1, tune=off)
+    assert info["fast_items"] == 0

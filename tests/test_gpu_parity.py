@@ -323,3 +323,18 @@ def test_multi_autotune(lib, tmp_path):
     r2 = pac.multi_autotune(lib, shapes, 2, 1, cache=cache)
     assert r2.cached == 1 and r2.tune.as_dict() == r.tune.as_dict()
     P.check_multi(lib, shapes, 1, stream=True, tune=r.tune.as_dict())
+
+
+
+@pytest.mark.parametrize("stream", [False, True])
+def test_multi_queue_fast_paths(lib, stream):
+    """Fused 2048-point rows and 512/256/128-point columns on the compile-time
+    bodies inside the work-queue kernel, against numpy per problem; with the
+    fast paths turned off (special = -1) the same results."""
+    shapes = [(2 ** 18,), (256, 2048), (512, 64), (2048,), (128, 2048), (2 ** 17,), (64, 32),
+              (2 ** 20,), (2048, 2048)]
+    cap11 = {"max_factor_log": 11, "max_radix_log": 0, "special": 0, "w_shift": 0}
+    info = P.check_multi(lib, shapes, 1, stream=stream, tune=cap11)
+    assert 0 < info["fast_items"] < sum(info["items"])
+    info = P.check_multi(lib, shapes, 1, stream=stream, tune=dict(cap11, special=-1))
+    assert info["fast_items"] == 0
