@@ -96,8 +96,10 @@ __global__ void __launch_bounds__(NT, MINB) pac_special_kernel(const PassDesc d)
 // is copied into shared memory (unless the CTA's previous item had the same
 // pass) and the CTA runs that pass's CTA `item - starts[k]` with the
 // run-time geometry of pac_pass_kernel.
+// (FP32: two CTAs per SM, the register bound the compile-time bodies are
+// written for; FP64 keeps one)
 template <typename T, int B2, int TC>
-__global__ void __launch_bounds__(256) pac_queue_kernel(const PassDesc* __restrict__ descs,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) pac_queue_kernel(const PassDesc* __restrict__ descs,
                                                         const long long* __restrict__ starts,
                                                         const int* __restrict__ item_desc,
                                                         long long total,

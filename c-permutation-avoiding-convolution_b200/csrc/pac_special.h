@@ -99,13 +99,13 @@ namespace pac {
 // fields: element type, bytes, log2 digit base, mode, sign, log2 L, column
 // tile, log2 W, tensor-core form
 #define PAC_QUEUE_LIST(X)                            \
-  X(float, 4, 1, MODE_CONV, 0, 11, 0, 1, 0)          \
+  X(float, 4, 1, MODE_CONV, 0, 11, 0, 2, 0)          \
   X(float, 4, 1, MODE_DIF, -1, 9, 1, 4, 0)           \
   X(float, 4, 1, MODE_DIT, +1, 9, 1, 4, 0)           \
-  X(float, 4, 1, MODE_DIF, -1, 8, 1, 4, 0)           \
-  X(float, 4, 1, MODE_DIT, +1, 8, 1, 4, 0)           \
-  X(float, 4, 1, MODE_DIF, -1, 7, 1, 5, 0)           \
-  X(float, 4, 1, MODE_DIT, +1, 7, 1, 5, 0)
+  X(float, 4, 1, MODE_DIF, -1, 8, 1, 5, 0)           \
+  X(float, 4, 1, MODE_DIT, +1, 8, 1, 5, 0)           \
+  X(float, 4, 1, MODE_DIF, -1, 7, 1, 6, 0)           \
+  X(float, 4, 1, MODE_DIT, +1, 7, 1, 6, 0)
 enum { PAC_QUEUE_THREADS = 256 };
 
 inline bool queue_geometry(int bytes, int b2, int mode, int sign, int logL, int cols, int tc,
