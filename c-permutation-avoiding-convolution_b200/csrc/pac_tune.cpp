@@ -177,7 +177,8 @@ struct TuneBufs {
 };
 
 // milliseconds per call of `run`: best of three rounds of enough calls to
-// fill ~10 ms, after two warm-up calls
+// fill ~10 ms (so microsecond-scale problems average over many launches),
+// after two warm-up calls
 template <class F>
 static int time_calls(F run, void* stream, double* ms) {
   void* e0 = nullptr;
@@ -191,7 +192,7 @@ static int time_calls(F run, void* stream, double* ms) {
   if (st == PAC_SUCCESS) st = be_event_record(e1, stream);
   if (st == PAC_SUCCESS) st = be_event_elapsed(e0, e1, &t);
   int reps = (int)ceil(10.0 / (t > 1e-3f ? t : 1e-3f));
-  reps = reps < 3 ? 3 : reps > 100 ? 100 : reps;
+  reps = reps < 3 ? 3 : reps > 2000 ? 2000 : reps;
   double best = 1e30;
   for (int round = 0; round < 3 && st == PAC_SUCCESS; ++round) {
     st = be_event_record(e0, stream);
