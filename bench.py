@@ -366,6 +366,16 @@ def run_ours(args, world, dist):
     peak, peak_kind = read_peaks()
     alg_bytes = 3 * batch * N * 2 * esz  # read x + read Hhat + write y
     achieved = alg_bytes / (ms_step * 1e-3) / 1e9
+    # arithmetic: two transforms of 5 N log2 N flops and the 6 N-flop product
+    # per problem, against the device's measured FMA throughput of the form's
+    # arithmetic type (FP32 for the tensor-core form's CUDA-core work)
+    flops = batch * (10.0 * N * np.log2(N) + 6.0 * N)
+    fma_tf = pac.fma_peak(L, esz, sp)
+    flop_rate = {"flops_per_step": flops, "achieved_tflops": round(flops / (ms_step * 1e-3) / 1e12, 3),
+                 "peak_tflops": round(fma_tf, 2),
+                 "frac": round(flops / (ms_step * 1e-3) / 1e12 / fma_tf, 4),
+                 "peak_source": f"measured: pac_fma_peak ({'FP64' if esz == 8 else 'FP32'} FMA "
+                                "chains, 8 per thread, 64 warps per SM)"}
     tot = sum(pass_ms) or 1.0
     passes = []
     for nm, pm in zip(pass_names(len(pass_ms)), pass_ms):
@@ -389,7 +399,8 @@ def run_ours(args, world, dist):
                       "l2": f"inputs larger than L2: x rotated over {R} buffers of "
                             f"{per / 2**20:.0f} MiB; Hhat {N * esz * 2 / 2**20:.0f} MiB",
                       "parallelism": f"replicas x{world}"},
-           "roofline": roofline, "gpu_launches": int(launches), "clocks": clocks,
+           "roofline": roofline, "flop_rate": flop_rate, "gpu_launches": int(launches),
+           "clocks": clocks,
            "filter_spectrum_ms": round(spectrum_ms, 4), "rel_l2_vs_numpy_fp64": max(errs),
            "max_err_vs_numpy_fp64": max(maxs)}
     out["config"]["l2_persisting_output"] = bool(l2_bytes)
@@ -864,7 +875,8 @@ def main():
         out["forms"] = {
             "f64": {"value": out["value"], "rel_l2_vs_numpy_fp64": out["rel_l2_vs_numpy_fp64"],
                     "max_err_vs_numpy_fp64": out["max_err_vs_numpy_fp64"],
-                    "roofline_frac": out["roofline"]["frac"]}}
+                    "roofline_frac": out["roofline"]["frac"],
+                    "flop_frac": out["flop_rate"]["frac"]}}
         for fm in ("f32", "tc"):
             af = argparse.Namespace(**vars(args))
             af.form = fm
@@ -873,7 +885,8 @@ def main():
                 "value": of["value"], "rel_l2_vs_numpy_fp64": of["rel_l2_vs_numpy_fp64"],
                 "max_err_vs_numpy_fp64": of["max_err_vs_numpy_fp64"],
                 "speedup_vs_f64": round(of["value"] / out["value"], 3),
-                "roofline_frac": of["roofline"]["frac"], "passes": of["roofline"]["passes"]}
+                "roofline_frac": of["roofline"]["frac"], "flop_frac": of["flop_rate"]["frac"],
+                "passes": of["roofline"]["passes"]}
     if rank == 0 and world == 1 and not args.no_cpu:
         procs = min(os.cpu_count() or 1, 16)
         pool = CpuPool(args.config, procs)

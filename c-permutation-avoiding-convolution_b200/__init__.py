@@ -91,6 +91,7 @@ def _declare(L):
     L.pac_stream_wait_stream.argtypes = [_vp, _vp]
     L.pac_stream_set_l2_persisting.argtypes = [_vp, _vp, sz]
     L.pac_launch_count.restype = ll
+    L.pac_fma_peak.argtypes = [i, _vp, C.POINTER(d)]
     L.pac_multi_create.argtypes = [C.POINTER(_vp), i, C.POINTER(i), C.POINTER(i), i, i]
     L.pac_multi_destroy.argtypes = [_vp]
     L.pac_multi_offsets.argtypes = [_vp, C.POINTER(ll)]
@@ -296,6 +297,13 @@ def autotune(L, dims, batch=1, digit_base=2, form=PAC_FORM_F64, stream=None, cac
     check(L, L.pac_autotune(len(dims), arr, bases, batch, form, stream,
                             cache.encode() if cache else None, C.byref(r)), "pac_autotune")
     return r
+
+
+def fma_peak(L, elem_bytes=8, stream=None):
+    """pac_fma_peak: measured FMA throughput of the device in TFLOP/s."""
+    v = C.c_double()
+    check(L, L.pac_fma_peak(elem_bytes, stream, C.byref(v)), "pac_fma_peak")
+    return v.value
 
 
 def multi_autotune(L, shapes, digit_base=2, form=PAC_FORM_F32, stream=None, cache=None):

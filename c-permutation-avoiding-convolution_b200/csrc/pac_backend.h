@@ -59,6 +59,8 @@ int be_scale_copy(long long n, int elem_bytes, const void* xr, const void* xi, v
                   void* yi, double scale, void* stream);
 int be_permute(long long n, const int* rho, double* re, double* im, void* stream);
 long long be_launch_count();
+// FMA throughput of the device (pac_fma_peak)
+int be_fma_peak(int elem_bytes, void* stream, double* tflops);
 
 // Persistent launch over a device work queue (pac_multi.cpp): the CTAs take
 // work items from *counter (zeroed beforehand) until `total` are done; item

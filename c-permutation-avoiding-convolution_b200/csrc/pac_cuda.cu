@@ -17,6 +17,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <atomic>
 #include <mutex>
 #include <set>
@@ -1041,5 +1042,57 @@ int be_permute(long long n, const int* rho, double* re, double* im, void* stream
 }
 
 long long be_launch_count() { return g_launches.load(); }
+
+// 8 independent FMA chains per thread; the result is stored only if it takes
+// a value the chains cannot reach, which keeps them live
+template <typename T>
+__global__ void __launch_bounds__(256) fma_peak_kernel(T* out, int iters, T a, T b) {
+  T x[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) x[k] = T(threadIdx.x + k) * T(1e-3);
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) x[k] = fma(x[k], a, b);
+  }
+  T s = 0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) s += x[k];
+  if (s == T(-1)) out[blockIdx.x] = s;
+}
+
+template <typename T>
+static int fma_peak_t(cudaStream_t st, double* tflops) {
+  const int iters = sizeof(T) == 8 ? 256 : 1024;
+  const long long blocks = 8LL * be_num_sms();
+  T* out = nullptr;
+  PAC_CU(cudaMalloc(&out, sizeof(T) * blocks), "cudaMalloc");
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  double best = 0;
+  cudaError_t err = cudaSuccess;
+  for (int r = 0; r < 4 && err == cudaSuccess; ++r) {
+    cudaEventRecord(e0, st);
+    fma_peak_kernel<T><<<(unsigned)blocks, 256, 0, st>>>(out, iters, T(0.999999), T(1e-7));
+    cudaEventRecord(e1, st);
+    err = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, e0, e1);
+    const double fl = 2.0 * 8.0 * iters * 256.0 * (double)blocks;
+    if (r > 0 && err == cudaSuccess && ms > 0.f) best = std::max(best, fl / (ms * 1e-3) / 1e12);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(out);
+  PAC_CU(err, "fma_peak_kernel");
+  g_launches.fetch_add(4, std::memory_order_relaxed);
+  *tflops = best;
+  return PAC_SUCCESS;
+}
+
+int be_fma_peak(int elem_bytes, void* stream, double* tflops) {
+  if (elem_bytes == 8) return fma_peak_t<double>((cudaStream_t)stream, tflops);
+  return fma_peak_t<float>((cudaStream_t)stream, tflops);
+}
 
 }  // namespace pac

@@ -409,6 +409,9 @@ int be_permute(long long n, const int* rho, double* re, double* im, void*) {
 }
 
 long long be_launch_count() { return g_launches.load(); }
+int be_fma_peak(int, void*, double*) {
+  return set_error(PAC_ERROR_NO_DEVICE, "pac_fma_peak: the host replay has no device to measure");
+}
 
 // work-queue launch: the items in queue order, one CTA each (the queue's
 // order is the one a single persistent CTA would take)

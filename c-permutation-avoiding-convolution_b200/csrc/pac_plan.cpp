@@ -1040,6 +1040,12 @@ PAC_API int pac_stream_wait_stream(pac_stream_t waiter, pac_stream_t waitee) {
   return be_stream_wait(waiter, waitee);
 }
 PAC_API long long pac_launch_count(void) { return be_launch_count(); }
+PAC_API int pac_fma_peak(int elem_bytes, pac_stream_t stream, double* tflops) {
+  if (!tflops || (elem_bytes != 8 && elem_bytes != 4))
+    return set_error(PAC_ERROR_INVALID_VALUE, "pac_fma_peak: elem_bytes 8 or 4, tflops non-NULL");
+  PAC_TRY(be_init());
+  return be_fma_peak(elem_bytes, stream, tflops);
+}
 
 PAC_API int pac_plan_set_pass_timing(pac_plan_t plan, int enable) {
   if (!plan) return set_error(PAC_ERROR_INVALID_VALUE, "pac_plan_set_pass_timing: NULL");

@@ -338,6 +338,13 @@ PAC_API int pac_plan_get_pass_timing(pac_plan_t plan, int max_passes, double* ms
 
 /* Number of this library's kernel launches since load (for accounting). */
 PAC_API long long pac_launch_count(void);
+/* The current device's measured arithmetic peak, the denominator of the
+ * flop-rate fraction bench.py reports beside the HBM roofline: a kernel of
+ * independent fused multiply-add chains (8 per thread, 8 CTAs of 256
+ * threads per SM), best of three timed launches on `stream`;
+ * *tflops = 2 x FMAs per second / 1e12.  elem_bytes 8: FP64, 4: FP32.
+ * No counterpart in the reference. */
+PAC_API int pac_fma_peak(int elem_bytes, pac_stream_t stream, double* tflops);
 
 PAC_API const char* pac_status_string(int status);
 /* Message of the last failed call on this host thread ("" if none). */

@@ -338,3 +338,11 @@ def test_multi_queue_fast_paths(lib, stream):
     assert 0 < info["fast_items"] < sum(info["items"])
     info = P.check_multi(lib, shapes, 1, stream=stream, tune=dict(cap11, special=-1))
     assert info["fast_items"] == 0
+
+
+
+def test_fma_peak(lib):
+    """pac_fma_peak: plausible B200 figures (FP64 tens of TFLOP/s, FP32 above it)."""
+    f64 = pac.fma_peak(lib, 8)
+    f32 = pac.fma_peak(lib, 4)
+    assert 5.0 < f64 < 200.0 and f32 > f64
