@@ -647,10 +647,11 @@ static int launch_special(const PassDesc& d, int elem_bytes, int b2, long long g
                           size_t smem, void* stream, bool* done) {
   *done = false;
   const int cols = d.logS > 0 ? 1 : 0;
+  int seen = 0;  // candidates of this geometry so far; d.spec - 1 picks one
 #define PAC_X(T, BY, B2_, MO, SG, LL, CO, LW, NT_, MB, TC_)                                   \
   if (!*done && elem_bytes == BY && b2 == B2_ && d.mode == MO &&                           \
-      (MO == MODE_CONV || d.sign == SG) && d.logL == LL && cols == CO && d.W == (1 << LW) && \
-      threads == NT_ && d.tc == TC_) {                                                     \
+      (MO == MODE_CONV || d.sign == SG) && d.logL == LL && cols == CO && d.tc == TC_ &&    \
+      seen++ == d.spec - 1 && d.W == (1 << LW) && threads == NT_) {                        \
     static std::mutex mu;                                                                  \
     static std::set<int> configured;                                                       \
     *done = true;                                                                          \

@@ -222,9 +222,11 @@ int be_launch_pass(const PassDesc& d, int elem_bytes, int b2, long long grid, in
   }
   if (d.spec) {
     const int cols = d.logS > 0 ? 1 : 0;
+    int seen = 0;  // candidates of this geometry so far; d.spec - 1 picks one
 #define PAC_X(T, BY, B2_, MO, SG, LL, CO, LW, NT_, MB, TC_)                                   \
   if (elem_bytes == BY && b2 == B2_ && d.mode == MO && (MO == MODE_CONV || d.sign == SG) && \
-      d.logL == LL && cols == CO && d.W == (1 << LW) && threads == NT_ && d.tc == TC_) {   \
+      d.logL == LL && cols == CO && d.tc == TC_ && seen++ == d.spec - 1 &&                 \
+      d.W == (1 << LW) && threads == NT_) {                                                 \
     replay_special<T, B2_, MO, SG, LL, CO, LW, NT_, TC_>(d, grid);                              \
     g_launches++;                                                                          \
     return PAC_SUCCESS;                                                                    \

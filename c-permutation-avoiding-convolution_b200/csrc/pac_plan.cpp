@@ -383,11 +383,12 @@ static void apply_special(const Schedule& s, PassSpec& p) {
     return;
   }
   const char* var = getenv("PAC_SPECIAL_VARIANT");
-  const int variant = s.special > 0 ? s.special : var ? atoi(var) : 0;
+  int variant = s.special > 0 ? s.special : var ? atoi(var) : 0;
   const int cols = d.logS > 0 ? 1 : 0;
-  if (!special_geometry(s.bytes, p.b2, d.mode, d.sign, d.logL, cols, d.tc, &logW, &nt, variant) &&
-      !special_geometry(s.bytes, p.b2, d.mode, d.sign, d.logL, cols, d.tc, &logW, &nt))
-    return;
+  if (!special_geometry(s.bytes, p.b2, d.mode, d.sign, d.logL, cols, d.tc, &logW, &nt, variant)) {
+    variant = 0;
+    if (!special_geometry(s.bytes, p.b2, d.mode, d.sign, d.logL, cols, d.tc, &logW, &nt)) return;
+  }
   const long long W = 1LL << logW;
   if ((d.nlines & (W - 1)) != 0) return;
   if (d.logS > 0 && logW > d.logS) return;
@@ -395,7 +396,7 @@ static void apply_special(const Schedule& s, PassSpec& p) {
   d.logW = logW;
   d.pitch = pitch_for(s.bytes, d.logL, d.W, cols, d.tc);
   d.nthreads = nt;
-  d.spec = 1;
+  d.spec = 1 + variant;
   p.threads = nt;
   p.grid = d.nlines / W;
   p.smem = (size_t)2 * d.W * d.pitch * s.bytes;

@@ -27,10 +27,6 @@ namespace pac {
   X(float, 4, 1, MODE_CONV, 0, 11, 0, 1, 256, 2, 0)           \
   X(float, 4, 1, MODE_DIF, -1, 11, 1, 3, 512, 1, 0)           \
   X(float, 4, 1, MODE_DIT, +1, 11, 1, 3, 512, 1, 0)           \
-  X(double, 8, 1, MODE_DIF, -1, 11, 1, 1, 256, 2, 0)          \
-  X(double, 8, 1, MODE_DIT, +1, 11, 1, 1, 256, 2, 0)          \
-  X(float, 4, 1, MODE_DIF, -1, 11, 1, 2, 512, 1, 0)           \
-  X(float, 4, 1, MODE_DIT, +1, 11, 1, 2, 512, 1, 0)           \
   /* 3D FP32: 256-point rows and columns (256^3, and the middle axis of */ \
   /* 512 x 256 x 128), 512-point columns and 128-point rows */           \
   X(float, 4, 1, MODE_CONV, 0, 8, 0, 4, 256, 2, 0)            \
@@ -39,18 +35,23 @@ namespace pac {
   X(float, 4, 1, MODE_DIF, -1, 9, 1, 4, 512, 1, 0)            \
   X(float, 4, 1, MODE_DIT, +1, 9, 1, 4, 512, 1, 0)            \
   X(float, 4, 1, MODE_CONV, 0, 7, 0, 5, 256, 2, 0)            \
+  /* second candidate (PAC_SPECIAL_VARIANT=1, tuner knob special = 1): */ \
+  /* the fused 2048-point FP32 pass at three CTAs per SM (85 registers, */ \
+  /* no spills; the FP64 pass at five CTAs spills 144 bytes) */             \
+  X(float, 4, 1, MODE_CONV, 0, 11, 0, 1, 256, 3, 0)           \
   /* tensor-core form, 2048-point rows and 8-line columns */             \
   X(float, 4, 1, MODE_CONV, 0, 11, 0, 1, 256, 2, 1)           \
   X(float, 4, 1, MODE_DIF, -1, 11, 1, 3, 512, 1, 1)           \
   X(float, 4, 1, MODE_DIT, +1, 11, 1, 3, 512, 1, 1)
 // Measured on C3 (2048^2): FP64 columns W=4 (32-byte rows) 53 us vs W=2
 // 68 us; FP32 columns W=8 34 us vs W=4 45 us -- row width, not occupancy,
-// bounds these passes.  On 3D 512 x 256 x 128 FP32 the specialised passes
+// bounds these passes (the narrower tiles were dropped from the list).  On 3D 512 x 256 x 128 FP32 the specialised passes
 // gain 4% over the generic kernel (256^3: 1%); specialising FP64 256-point
 // passes and the base-4 4096/16-point passes of 1D 2^16 measured 2-5%
 // slower than the generic kernel, so those shapes stay generic.
 // (a geometry may have several candidates; the first is the default and
-// PAC_SPECIAL_VARIANT=k selects the k-th, for tuning)
+// PAC_SPECIAL_VARIANT=k or the tuner knob special = k selects the k-th; the
+// pass descriptor records it as spec = 1 + k)
 
 // Column passes whose tile is shared by a cluster of 2^logC CTAs
 // (PassDesc.logC, pass_body_cl): each CTA holds L / 2^logC rows of the

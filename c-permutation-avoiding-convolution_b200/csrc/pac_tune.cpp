@@ -4,8 +4,9 @@
 // the tuner allocates (contents irrelevant to the time: zeros), one plan per
 // candidate knob set, each timed with device events as the best of three
 // rounds of enough calls to fill ~10 ms.  The search is a coordinate
-// descent from the built-in knobs over (specialised kernels off, radix 8
-// stages, shorter factors, narrower / wider generic tiles); a step is kept
+// descent from the built-in knobs over (specialised kernels off or their
+// second candidates, radix 8 stages, shorter factors, narrower / wider
+// generic tiles); a step is kept
 // only if it is at least 2% faster, so timing noise does not move a plan
 // off the built-in choices.  Candidates that build the same schedule as one
 // already timed (a factor cap that splits no axis differently) are skipped.
@@ -233,9 +234,12 @@ static void descend(M measure, bool search_special, int bytes, pac_tune_result_t
     return false;
   };
   if (search_special) {
-    pac_tune_t t = cur;
-    t.special = -1;
-    consider(t, false);
+    const pac_tune_t base = cur;
+    for (int sp : {-1, 1}) {  // generic kernels only; the second specialised candidates
+      pac_tune_t t = base;
+      t.special = sp;
+      consider(t, false);
+    }
   }
   {
     pac_tune_t t = cur;
