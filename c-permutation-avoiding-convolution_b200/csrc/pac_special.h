@@ -24,7 +24,7 @@ namespace pac {
   X(double, 8, 1, MODE_CONV, 0, 11, 0, 0, 128, 4, 0)          \
   X(double, 8, 1, MODE_DIF, -1, 11, 1, 2, 512, 1, 0)          \
   X(double, 8, 1, MODE_DIT, +1, 11, 1, 2, 512, 1, 0)          \
-  X(float, 4, 1, MODE_CONV, 0, 11, 0, 1, 256, 2, 0)           \
+  X(float, 4, 1, MODE_CONV, 0, 11, 0, 1, 256, 3, 0)           \
   X(float, 4, 1, MODE_DIF, -1, 11, 1, 3, 512, 1, 0)           \
   X(float, 4, 1, MODE_DIT, +1, 11, 1, 3, 512, 1, 0)           \
   /* 3D FP32: 256-point rows and columns (256^3, and the middle axis of */ \
@@ -36,9 +36,10 @@ namespace pac {
   X(float, 4, 1, MODE_DIT, +1, 9, 1, 4, 512, 1, 0)            \
   X(float, 4, 1, MODE_CONV, 0, 7, 0, 5, 256, 2, 0)            \
   /* second candidate (PAC_SPECIAL_VARIANT=1, tuner knob special = 1): */ \
-  /* the fused 2048-point FP32 pass at three CTAs per SM (85 registers, */ \
-  /* no spills; the FP64 pass at five CTAs spills 144 bytes) */             \
-  X(float, 4, 1, MODE_CONV, 0, 11, 0, 1, 256, 3, 0)           \
+  /* the fused 2048-point FP32 pass at two CTAs per SM (128 registers); */ \
+  /* three (85 registers, no spills) measured 34.9 against 37.2 us on */   \
+  /* 2048^2; the FP64 pass at five CTAs per SM spills 144 bytes */         \
+  X(float, 4, 1, MODE_CONV, 0, 11, 0, 1, 256, 2, 0)           \
   /* tensor-core form, 2048-point rows and 8-line columns */             \
   X(float, 4, 1, MODE_CONV, 0, 11, 0, 1, 256, 2, 1)           \
   X(float, 4, 1, MODE_DIF, -1, 11, 1, 3, 512, 1, 1)           \
