@@ -46,7 +46,9 @@ namespace pac {
   X(float, 4, 1, MODE_DIT, +1, 11, 1, 3, 512, 1, 1)
 // Measured on C3 (2048^2): FP64 columns W=4 (32-byte rows) 53 us vs W=2
 // 68 us; FP32 columns W=8 34 us vs W=4 45 us -- row width, not occupancy,
-// bounds these passes (the narrower tiles were dropped from the list).  On 3D 512 x 256 x 128 FP32 the specialised passes
+// bounds these passes (the narrower tiles were dropped from the list), and
+// neither do more warps: FP32 columns at 1024 threads per CTA (64 registers,
+// no spills) ran 30.0 / 30.6 us against 31.2 / 30.1 us.  On 3D 512 x 256 x 128 FP32 the specialised passes
 // gain 4% over the generic kernel (256^3: 1%); specialising FP64 256-point
 // passes and the base-4 4096/16-point passes of 1D 2^16 measured 2-5%
 // slower than the generic kernel, so those shapes stay generic.
