@@ -24,7 +24,7 @@ namespace pac {
   X(double, 8, 1, MODE_CONV, 0, 11, 0, 0, 128, 4, 0)          \
   X(double, 8, 1, MODE_DIF, -1, 11, 1, 2, 512, 1, 0)          \
   X(double, 8, 1, MODE_DIT, +1, 11, 1, 2, 512, 1, 0)          \
-  X(float, 4, 1, MODE_CONV, 0, 11, 0, 1, 256, 3, 0)           \
+  X(float, 4, 1, MODE_CONV, 0, 11, 0, 1, 256, 4, 0)           \
   X(float, 4, 1, MODE_DIF, -1, 11, 1, 3, 512, 1, 0)           \
   X(float, 4, 1, MODE_DIT, +1, 11, 1, 3, 512, 1, 0)           \
   /* 3D FP32: 256-point rows and columns (256^3, and the middle axis of */ \
@@ -35,10 +35,11 @@ namespace pac {
   X(float, 4, 1, MODE_DIF, -1, 9, 1, 4, 512, 2, 0)            \
   X(float, 4, 1, MODE_DIT, +1, 9, 1, 4, 512, 2, 0)            \
   X(float, 4, 1, MODE_CONV, 0, 7, 0, 5, 256, 3, 0)            \
-  /* second candidate (PAC_SPECIAL_VARIANT=1, tuner knob special = 1): */ \
-  /* the fused 2048-point FP32 pass at two CTAs per SM (128 registers); */ \
-  /* three (85 registers, no spills) measured 34.9 against 37.2 us on */   \
-  /* 2048^2; the FP64 pass at five CTAs per SM spills 144 bytes */         \
+  /* further candidates (PAC_SPECIAL_VARIANT=k, tuner knob special = k): */ \
+  /* the fused 2048-point FP32 pass at three and two CTAs per SM; on */      \
+  /* 2048^2 four (64 registers, no spills) ran 33.2 us, three 34.9, two */   \
+  /* 37.2; the FP64 pass at five CTAs per SM spills 144 bytes */              \
+  X(float, 4, 1, MODE_CONV, 0, 11, 0, 1, 256, 3, 0)           \
   X(float, 4, 1, MODE_CONV, 0, 11, 0, 1, 256, 2, 0)           \
   /* the 3D passes at the other occupancy: on 512 x 256 x 128 the */     \
   /* 512-point columns at 2 CTAs per SM ran 145 / 135 us against 149 / */ \
