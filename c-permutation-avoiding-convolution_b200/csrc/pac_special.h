@@ -35,6 +35,9 @@ namespace pac {
   X(float, 4, 1, MODE_DIF, -1, 9, 1, 4, 512, 2, 0)            \
   X(float, 4, 1, MODE_DIT, +1, 9, 1, 4, 512, 2, 0)            \
   X(float, 4, 1, MODE_CONV, 0, 7, 0, 5, 256, 3, 0)            \
+  /* 1D batches: fused 4096-point rows (2^16-point lines split 16 x 4096) */ \
+  X(float, 4, 1, MODE_CONV, 0, 12, 0, 1, 256, 3, 0)           \
+  X(double, 8, 1, MODE_CONV, 0, 12, 0, 0, 256, 2, 0)          \
   /* further candidates (PAC_SPECIAL_VARIANT=k, tuner knob special = k): */ \
   /* the fused 2048-point FP32 pass at three and two CTAs per SM; on */      \
   /* 2048^2 four (64 registers, no spills) ran 33.2 us, three 34.9, two */   \

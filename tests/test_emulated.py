@@ -45,7 +45,9 @@ def test_multi_factor_splits(emu, orc, cap, monkeypatch):
     # 512-point columns and 128-point rows, base-4 4096-point rows and
     # 16-point columns
     ((256, 16, 256), 1, 2, 1, False), ((256, 8, 256), 1, 2, 0, False),
-    ((512, 2, 128), 1, 2, 1, False), ((2 ** 16,), 2, 4, 0, False), ((2 ** 16,), 2, 4, 1, False)])
+    ((512, 2, 128), 1, 2, 1, False), ((2 ** 16,), 2, 4, 0, False), ((2 ** 16,), 2, 4, 1, False),
+    # fused 4096-point rows (FP64 one line per CTA, FP32 two)
+    ((4096,), 2, 2, 0, False), ((4096,), 4, 2, 1, True), ((16, 4096), 2, 2, 1, False)])
 def test_native_conv(emu, dims, batch, base, form, per):
     g = rng(21)
     shape = (batch,) + dims
