@@ -423,7 +423,16 @@ static void apply_queue_special(const Schedule& s, PassSpec& p) {
   p.smem = (size_t)2 * d.W * d.pitch * s.bytes;
 }
 
+// A pass of one stage reads global memory into registers and writes them
+// back (no exchange through shared memory, unless it stores in natural order
+// out of shared memory): it reserves none, so more CTAs fit per SM.
+static size_t pass_smem(const PassSpec& p) {
+  const PassDesc& d = p.d;
+  return (d.nst == 1 && !d.nat && !d.pipe && d.logC == 0) ? 0 : p.smem;
+}
+
 static int launch(const Schedule& s, PassSpec& p, void* stream) {
+  p.smem = pass_smem(p);
   return be_launch_pass(p.d, s.bytes, p.b2, p.grid, p.threads, p.smem, stream);
 }
 
@@ -627,6 +636,7 @@ int plan_conv_descs(pac_plan_s* pl, const void* x_re, const void* x_im, const vo
     build_conv_passes(pl, x_re, x_im, h_re, h_im, 0, y_re, y_im, 1.0, passes);
   for (auto& p : passes) apply_queue_special(pl->main, p);
   for (auto& p : passes) {
+    p.smem = pass_smem(p);
     descs.push_back(p.d);
     ctas.push_back(p.grid);
     smem.push_back(p.smem);

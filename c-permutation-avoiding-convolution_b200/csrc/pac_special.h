@@ -35,6 +35,11 @@ namespace pac {
   X(float, 4, 1, MODE_DIF, -1, 9, 1, 4, 512, 2, 0)            \
   X(float, 4, 1, MODE_DIT, +1, 9, 1, 4, 512, 2, 0)            \
   X(float, 4, 1, MODE_CONV, 0, 7, 0, 5, 256, 3, 0)            \
+  /* 1D batches: 16-point columns (one radix-16 stage, no shared memory) */ \
+  X(float, 4, 1, MODE_DIF, -1, 4, 1, 8, 256, 4, 0)            \
+  X(float, 4, 1, MODE_DIT, +1, 4, 1, 8, 256, 4, 0)            \
+  X(double, 8, 1, MODE_DIF, -1, 4, 1, 8, 256, 2, 0)           \
+  X(double, 8, 1, MODE_DIT, +1, 4, 1, 8, 256, 2, 0)           \
   /* 1D batches: fused 4096-point rows (2^16-point lines split 16 x 4096) */ \
   X(float, 4, 1, MODE_CONV, 0, 12, 0, 1, 256, 3, 0)           \
   X(double, 8, 1, MODE_CONV, 0, 12, 0, 0, 256, 2, 0)          \

@@ -128,8 +128,10 @@ def test_c4_3d_f64_against_oracle(lib, orc):
     ((256, 16, 256), 1, 2, 1, False), ((256, 8, 256), 1, 2, 0, False),
     ((512, 2, 128), 1, 2, 1, False), ((2 ** 16,), 2, 4, 0, False), ((2 ** 16,), 2, 4, 1, False),
     ((2 ** 20,), 2, 2, 0, False), ((2 ** 20,), 2, 2, 1, False),
-    # fused 4096-point rows (FP64 one line per CTA, FP32 two)
-    ((4096,), 2, 2, 0, False), ((4096,), 4, 2, 1, True), ((16, 4096), 2, 2, 1, False)])
+    # fused 4096-point rows (FP64 one line per CTA, FP32 two); 16-point
+    # columns of 256-column tiles (2^16 = 16 x 4096, a 16 x 8192 plane)
+    ((4096,), 2, 2, 0, False), ((4096,), 4, 2, 1, True), ((16, 4096), 2, 2, 1, False),
+    ((2 ** 16,), 8, 2, 0, False), ((2 ** 16,), 8, 2, 1, False), ((16, 8192), 1, 2, 0, False)])
 def test_native_conv(lib, dims, batch, base, form, per):
     g = rng(21)
     shape = (batch,) + dims
