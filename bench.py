@@ -286,10 +286,12 @@ def run_ours(args, world, dist):
     sp = stream.cuda_stream
     # tuning first, with no L2 window set: every candidate is timed alike
     tuned = tune_workload(L, args, dims, batch, form, sp)
+    knobs = parse_knobs(args.knobs)
     l2_bytes = ybuf.numel() * ybuf.element_size() if args.l2 == "on" else 0
     if l2_bytes:
         pac.check(L, L.pac_stream_set_l2_persisting(sp, ybuf.data_ptr(), l2_bytes), "l2")
-    plan = pac.Plan(L, dims, batch, 2, form)  # the tuned knobs, through PAC_TUNE_CACHE
+    # the tuned knobs (through PAC_TUNE_CACHE), or --knobs
+    plan = pac.Plan(L, dims, batch, 2, form, tune=knobs)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     plan.filter_spectrum(hd[0].data_ptr(), hd[1].data_ptr(), Hh[0].data_ptr(), Hh[1].data_ptr(),
@@ -405,6 +407,8 @@ def run_ours(args, world, dist):
            "max_err_vs_numpy_fp64": max(maxs)}
     out["config"]["l2_persisting_output"] = bool(l2_bytes)
     out["config"]["autotune"] = tuned
+    if knobs is not None:
+        out["config"]["knobs"] = knobs
     if l2_bytes:
         pac.check(L, L.pac_stream_set_l2_persisting(sp, None, 0), "l2")
     plan.close()
@@ -457,10 +461,23 @@ def _tune_record(r):
             "cache": os.environ.get("PAC_TUNE_CACHE")}
 
 
+def parse_knobs(text):
+    """--knobs "max_radix_log=3,w_shift=1": explicit pac_tune_t knobs (the rest 0)."""
+    if not text:
+        return None
+    knobs = {"max_factor_log": 0, "max_radix_log": 0, "special": 0, "w_shift": 0}
+    for item in text.split(","):
+        k, v = item.split("=")
+        if k.strip() not in knobs:
+            raise SystemExit(f"--knobs: unknown knob {k!r} (known: {', '.join(knobs)})")
+        knobs[k.strip()] = int(v)
+    return knobs
+
+
 def tune_workload(L, args, dims, batch, form, sp):
     """pac_autotune for the workload (before anything is timed); the result
     lands in PAC_TUNE_CACHE, which every plan this process creates reads."""
-    if args.tune != "on":
+    if args.tune != "on" or args.knobs:
         return None
     return _tune_record(pac.autotune(L, dims, batch, 2, form, stream=sp,
                                      cache=os.environ["PAC_TUNE_CACHE"]))
@@ -828,6 +845,9 @@ def main():
     ap.add_argument("--tune", choices=["on", "off"], default="on",
                     help="autotune the plan knobs (pac_autotune) before timing; the cache is "
                          "PAC_TUNE_CACHE if set, else a fresh file for this run")
+    ap.add_argument("--knobs", default="",
+                    help="explicit plan knobs for the timed plan, e.g. max_radix_log=3,w_shift=1 "
+                         "(no tuning)")
     ap.add_argument("--l2", choices=["on", "off"], default="on",
                     help="keep the output (the passes' intermediate) L2-persisting")
     ap.add_argument("--profile", action="store_true",

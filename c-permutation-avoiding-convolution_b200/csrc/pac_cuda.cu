@@ -76,7 +76,7 @@ __global__ void __launch_bounds__(256) pac_pass_kernel(const PassDesc d) {
 // A pass compiled for one geometry (pac_special.h): tile W = 2^LOGW lines of
 // 2^LOGL elements, NT threads, register bound for MINB CTAs per SM.
 template <typename T, int B2, int MODE, int SIGN, int LOGL, int COLS, int LOGW, int NT, int MINB,
-          int TC>
+          int TC, int RC>
 __global__ void __launch_bounds__(NT, MINB) pac_special_kernel(const PassDesc d) {
   constexpr int W = 1 << LOGW;
   constexpr int PITCH = pitch_for((int)sizeof(T), LOGL, W, COLS, TC);
@@ -88,7 +88,7 @@ __global__ void __launch_bounds__(NT, MINB) pac_special_kernel(const PassDesc d)
   const long long cta = blockIdx.x;
   if ((int)threadIdx.x < W) s_lb[threadIdx.x] = line_base(d, cta * W + threadIdx.x);
   __syncthreads();
-  pass_body_ct<T, B2, MODE, SIGN, SP, NT, RadsFor<LOGL, B2>, TC>(d, cta, sre, sim, s_lb, s_lb);
+  pass_body_ct<T, B2, MODE, SIGN, SP, NT, RadsCap<LOGL, B2, RC>, TC>(d, cta, sre, sim, s_lb, s_lb);
 }
 
 // Persistent CTAs over a device work queue (many passes of different
@@ -648,15 +648,16 @@ static int launch_special(const PassDesc& d, int elem_bytes, int b2, long long g
   *done = false;
   const int cols = d.logS > 0 ? 1 : 0;
   int seen = 0;  // candidates of this geometry so far; d.spec - 1 picks one
-#define PAC_X(T, BY, B2_, MO, SG, LL, CO, LW, NT_, MB, TC_)                                   \
+#define PAC_X(T, BY, B2_, MO, SG, LL, CO, LW, NT_, MB, TC_, RC_)                              \
   if (!*done && elem_bytes == BY && b2 == B2_ && d.mode == MO &&                           \
       (MO == MODE_CONV || d.sign == SG) && d.logL == LL && cols == CO && d.tc == TC_ &&    \
-      seen++ == d.spec - 1 && d.W == (1 << LW) && threads == NT_) {                        \
+      rads_match(d, LL, B2_, RC_) && seen++ == d.spec - 1 && d.W == (1 << LW) &&           \
+      threads == NT_) {                                                                    \
     static std::mutex mu;                                                                  \
     static std::set<int> configured;                                                       \
     *done = true;                                                                          \
-    return launch_kernel(pac_special_kernel<T, B2_, MO, SG, LL, CO, LW, NT_, MB, TC_>, d,   \
-                         grid, threads, smem, stream, configured, mu);                     \
+    return launch_kernel(pac_special_kernel<T, B2_, MO, SG, LL, CO, LW, NT_, MB, TC_, RC_>, \
+                         d, grid, threads, smem, stream, configured, mu);                  \
   }
   PAC_SPECIAL_LIST(PAC_X)
 #undef PAC_X

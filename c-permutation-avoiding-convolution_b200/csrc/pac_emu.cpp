@@ -98,7 +98,8 @@ static void replay(const PassDesc& d, long long grid) {
 }
 
 // replay of a specialised kernel (pac_special.h): the compile-time body
-template <typename T, int B2, int MODE, int SIGN, int LOGL, int COLS, int LOGW, int NT, int TC>
+template <typename T, int B2, int MODE, int SIGN, int LOGL, int COLS, int LOGW, int NT, int TC,
+          int RC>
 static void replay_special(const PassDesc& d, long long grid) {
   constexpr int W = 1 << LOGW;
   constexpr int PITCH = pitch_for((int)sizeof(T), LOGL, W, COLS, TC);
@@ -107,7 +108,7 @@ static void replay_special(const PassDesc& d, long long grid) {
   std::vector<long long> lb(W);
   for (long long cta = 0; cta < grid; ++cta) {
     for (int w = 0; w < W; ++w) lb[w] = line_base(d, cta * W + w);
-    pass_body_ct<T, B2, MODE, SIGN, SP, NT, RadsFor<LOGL, B2>, TC>(
+    pass_body_ct<T, B2, MODE, SIGN, SP, NT, RadsCap<LOGL, B2, RC>, TC>(
         d, cta, sm.data(), sm.data() + (size_t)W * PITCH, lb.data(), lb.data());
   }
 }
@@ -223,11 +224,11 @@ int be_launch_pass(const PassDesc& d, int elem_bytes, int b2, long long grid, in
   if (d.spec) {
     const int cols = d.logS > 0 ? 1 : 0;
     int seen = 0;  // candidates of this geometry so far; d.spec - 1 picks one
-#define PAC_X(T, BY, B2_, MO, SG, LL, CO, LW, NT_, MB, TC_)                                   \
+#define PAC_X(T, BY, B2_, MO, SG, LL, CO, LW, NT_, MB, TC_, RC_)                              \
   if (elem_bytes == BY && b2 == B2_ && d.mode == MO && (MO == MODE_CONV || d.sign == SG) && \
-      d.logL == LL && cols == CO && d.tc == TC_ && seen++ == d.spec - 1 &&                 \
-      d.W == (1 << LW) && threads == NT_) {                                                 \
-    replay_special<T, B2_, MO, SG, LL, CO, LW, NT_, TC_>(d, grid);                              \
+      d.logL == LL && cols == CO && d.tc == TC_ && rads_match(d, LL, B2_, RC_) &&          \
+      seen++ == d.spec - 1 && d.W == (1 << LW) && threads == NT_) {                         \
+    replay_special<T, B2_, MO, SG, LL, CO, LW, NT_, TC_, RC_>(d, grid);                              \
     g_launches++;                                                                          \
     return PAC_SUCCESS;                                                                    \
   }

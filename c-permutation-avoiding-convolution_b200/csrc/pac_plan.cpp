@@ -109,14 +109,8 @@ static const int kSmemBudget = 200 * 1024;
 // bits (the same rule: fewest stages, bits spread evenly, larger first)
 static std::vector<int> radix_schedule(int lg, int b2, int rlog_cap = 4) {
   std::vector<int> r;
-  if (rlog_cap >= 4 || b2 == 3) {
-    for (int i = 0; i < sched_n(lg, b2); ++i) r.push_back(sched_v(lg, b2, i));
-    return r;
-  }
-  const int per = rlog_cap / b2 > 0 ? rlog_cap / b2 : 1;  // digits per stage at most
-  const int digits = lg / b2;
-  const int n = (digits + per - 1) / per;
-  for (int i = 0; i < n; ++i) r.push_back((digits / n + (i < digits % n ? 1 : 0)) * b2);
+  for (int i = 0; i < sched_n_cap(lg, b2, rlog_cap); ++i)
+    r.push_back(sched_v_cap(lg, b2, rlog_cap, i));
   return r;
 }
 
@@ -337,14 +331,13 @@ static void apply_special(const Schedule& s, PassSpec& p) {
   PassDesc& d = p.d;
   int logW = 0, nt = 0;
   if (d.nat) return;
-  // tuned off, or a radix schedule other than the one the specialised
-  // kernels are compiled with
-  if (s.special < 0 || s.rlog_cap < 4) return;
+  if (s.special < 0) return;  // tuned off
   // column pass whose tile a CTA cluster shares (W columns within the
   // stride, whole tiles), opt-in: PAC_CLUSTER_VARIANT=k picks the k-th
   // candidate geometry of the cluster list
   // (the cluster and pipelined variants have no tensor-core stages)
-  const char* cvar = d.tc ? nullptr : getenv("PAC_CLUSTER_VARIANT");
+  // (the cluster and pipelined variants run the radix-16 schedule only)
+  const char* cvar = d.tc || s.rlog_cap < 4 ? nullptr : getenv("PAC_CLUSTER_VARIANT");
   if (d.logS > 0 && cvar != nullptr) {
     int logC = 0;
     if (cluster_geometry(s.bytes, p.b2, d.mode, d.sign, d.logL, &logW, &logC, &nt, atoi(cvar)) &&
@@ -364,7 +357,7 @@ static void apply_special(const Schedule& s, PassSpec& p) {
   // pipelined column pass, opt-in (PAC_PIPE=1): persistent CTAs, one per
   // SM, tensor-copy prefetch of the next tile (16-byte aligned input arrays
   // for the tensor maps)
-  const char* pipe = d.tc ? nullptr : getenv("PAC_PIPE");
+  const char* pipe = d.tc || s.rlog_cap < 4 ? nullptr : getenv("PAC_PIPE");
   if (d.logS > 0 && cvar == nullptr && pipe != nullptr && atoi(pipe) != 0 &&
       pipe_geometry(s.bytes, p.b2, d.mode, d.sign, d.logL, &logW, &nt) && logW <= d.logS &&
       (d.nlines & ((1LL << logW) - 1)) == 0 && (d.nlines >> d.logS) < (1LL << 31) &&
@@ -385,9 +378,12 @@ static void apply_special(const Schedule& s, PassSpec& p) {
   const char* var = getenv("PAC_SPECIAL_VARIANT");
   int variant = s.special > 0 ? s.special : var ? atoi(var) : 0;
   const int cols = d.logS > 0 ? 1 : 0;
-  if (!special_geometry(s.bytes, p.b2, d.mode, d.sign, d.logL, cols, d.tc, &logW, &nt, variant)) {
+  const int rc = s.rlog_cap < 4 ? s.rlog_cap : 4;
+  if (!special_geometry(s.bytes, p.b2, d.mode, d.sign, d.logL, cols, d.tc, rc, &logW, &nt,
+                        variant)) {
     variant = 0;
-    if (!special_geometry(s.bytes, p.b2, d.mode, d.sign, d.logL, cols, d.tc, &logW, &nt)) return;
+    if (!special_geometry(s.bytes, p.b2, d.mode, d.sign, d.logL, cols, d.tc, rc, &logW, &nt))
+      return;
   }
   const long long W = 1LL << logW;
   if ((d.nlines & (W - 1)) != 0) return;

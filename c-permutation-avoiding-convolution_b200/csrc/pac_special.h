@@ -19,55 +19,61 @@ namespace pac {
 
 // fields: element type, bytes, log2 digit base, mode, sign (DIF/DIT), log2 L,
 // column tile (element stride > 1), log2 W, threads, min CTAs per SM,
-// tensor-core form (radix-16 stages on the tensor cores, pac_tc.cuh)
+// tensor-core form (radix-16 stages on the tensor cores, pac_tc.cuh), log2
+// of the largest stage radix (4: the default schedule RadsFor; 3: radix 8,
+// for plans tuned with max_radix_log = 3, RadsCap)
 #define PAC_SPECIAL_LIST(X)                                \
-  X(double, 8, 1, MODE_CONV, 0, 11, 0, 0, 128, 4, 0)          \
-  X(double, 8, 1, MODE_DIF, -1, 11, 1, 2, 512, 1, 0)          \
-  X(double, 8, 1, MODE_DIT, +1, 11, 1, 2, 512, 1, 0)          \
-  X(float, 4, 1, MODE_CONV, 0, 11, 0, 1, 256, 4, 0)           \
-  X(float, 4, 1, MODE_DIF, -1, 11, 1, 3, 512, 1, 0)           \
-  X(float, 4, 1, MODE_DIT, +1, 11, 1, 3, 512, 1, 0)           \
+  X(double, 8, 1, MODE_CONV, 0, 11, 0, 0, 128, 4, 0, 4)          \
+  X(double, 8, 1, MODE_DIF, -1, 11, 1, 2, 512, 1, 0, 4)          \
+  X(double, 8, 1, MODE_DIT, +1, 11, 1, 2, 512, 1, 0, 4)          \
+  X(float, 4, 1, MODE_CONV, 0, 11, 0, 1, 256, 4, 0, 4)           \
+  X(float, 4, 1, MODE_DIF, -1, 11, 1, 3, 512, 1, 0, 4)           \
+  X(float, 4, 1, MODE_DIT, +1, 11, 1, 3, 512, 1, 0, 4)           \
   /* 3D FP32: 256-point rows and columns (256^3, and the middle axis of */ \
   /* 512 x 256 x 128), 512-point columns and 128-point rows */           \
-  X(float, 4, 1, MODE_CONV, 0, 8, 0, 4, 256, 3, 0)            \
-  X(float, 4, 1, MODE_DIF, -1, 8, 1, 4, 256, 2, 0)            \
-  X(float, 4, 1, MODE_DIT, +1, 8, 1, 4, 256, 2, 0)            \
-  X(float, 4, 1, MODE_DIF, -1, 9, 1, 4, 512, 2, 0)            \
-  X(float, 4, 1, MODE_DIT, +1, 9, 1, 4, 512, 2, 0)            \
-  X(float, 4, 1, MODE_CONV, 0, 7, 0, 5, 256, 3, 0)            \
+  X(float, 4, 1, MODE_CONV, 0, 8, 0, 4, 256, 3, 0, 4)            \
+  X(float, 4, 1, MODE_DIF, -1, 8, 1, 4, 256, 2, 0, 4)            \
+  X(float, 4, 1, MODE_DIT, +1, 8, 1, 4, 256, 2, 0, 4)            \
+  X(float, 4, 1, MODE_DIF, -1, 9, 1, 4, 512, 2, 0, 4)            \
+  X(float, 4, 1, MODE_DIT, +1, 9, 1, 4, 512, 2, 0, 4)            \
+  X(float, 4, 1, MODE_CONV, 0, 7, 0, 5, 256, 3, 0, 4)            \
   /* 1D batches: 16-point columns (one radix-16 stage, no shared memory) */ \
-  X(float, 4, 1, MODE_DIF, -1, 4, 1, 8, 256, 4, 0)            \
-  X(float, 4, 1, MODE_DIT, +1, 4, 1, 8, 256, 4, 0)            \
-  X(double, 8, 1, MODE_DIF, -1, 4, 1, 8, 256, 2, 0)           \
-  X(double, 8, 1, MODE_DIT, +1, 4, 1, 8, 256, 2, 0)           \
+  X(float, 4, 1, MODE_DIF, -1, 4, 1, 8, 256, 4, 0, 4)            \
+  X(float, 4, 1, MODE_DIT, +1, 4, 1, 8, 256, 4, 0, 4)            \
+  X(double, 8, 1, MODE_DIF, -1, 4, 1, 8, 256, 2, 0, 4)           \
+  X(double, 8, 1, MODE_DIT, +1, 4, 1, 8, 256, 2, 0, 4)           \
   /* 1D batches: fused 4096-point rows (2^16-point lines split 16 x 4096) */ \
-  X(float, 4, 1, MODE_CONV, 0, 12, 0, 1, 256, 3, 0)           \
-  X(double, 8, 1, MODE_CONV, 0, 12, 0, 0, 256, 2, 0)          \
+  X(float, 4, 1, MODE_CONV, 0, 12, 0, 1, 256, 3, 0, 4)           \
+  X(double, 8, 1, MODE_CONV, 0, 12, 0, 0, 256, 2, 0, 4)          \
   /* further candidates (PAC_SPECIAL_VARIANT=k, tuner knob special = k): */ \
   /* the fused 2048-point FP32 pass at three and two CTAs per SM; on */      \
   /* 2048^2 four (64 registers, no spills) ran 33.2 us, three 34.9, two */   \
   /* 37.2; the FP64 pass at five CTAs per SM spills 144 bytes */              \
-  X(float, 4, 1, MODE_CONV, 0, 11, 0, 1, 256, 3, 0)           \
-  X(float, 4, 1, MODE_CONV, 0, 11, 0, 1, 256, 2, 0)           \
+  X(float, 4, 1, MODE_CONV, 0, 11, 0, 1, 256, 3, 0, 4)           \
+  X(float, 4, 1, MODE_CONV, 0, 11, 0, 1, 256, 2, 0, 4)           \
   /* the 3D passes at the other occupancy: on 512 x 256 x 128 the */     \
   /* 512-point columns at 2 CTAs per SM ran 145 / 135 us against 149 / */ \
   /* 151 at one, the fused 128-point rows at 3 CTAs 155 against 160 us; */ \
   /* 256-point columns at 3 CTAs were 2-7% slower (not kept) */           \
-  X(float, 4, 1, MODE_CONV, 0, 8, 0, 4, 256, 2, 0)            \
-  X(float, 4, 1, MODE_DIF, -1, 9, 1, 4, 512, 1, 0)            \
-  X(float, 4, 1, MODE_DIT, +1, 9, 1, 4, 512, 1, 0)            \
-  X(float, 4, 1, MODE_CONV, 0, 7, 0, 5, 256, 2, 0)            \
+  X(float, 4, 1, MODE_CONV, 0, 8, 0, 4, 256, 2, 0, 4)            \
+  X(float, 4, 1, MODE_DIF, -1, 9, 1, 4, 512, 1, 0, 4)            \
+  X(float, 4, 1, MODE_DIT, +1, 9, 1, 4, 512, 1, 0, 4)            \
+  X(float, 4, 1, MODE_CONV, 0, 7, 0, 5, 256, 2, 0, 4)            \
   /* tensor-core form, 2048-point rows and 8-line columns */             \
-  X(float, 4, 1, MODE_CONV, 0, 11, 0, 1, 256, 3, 1)           \
-  X(float, 4, 1, MODE_DIF, -1, 11, 1, 3, 512, 1, 1)           \
-  X(float, 4, 1, MODE_DIT, +1, 11, 1, 3, 512, 1, 1)           \
+  X(float, 4, 1, MODE_CONV, 0, 11, 0, 1, 256, 3, 1, 4)           \
+  X(float, 4, 1, MODE_DIF, -1, 11, 1, 3, 512, 1, 1, 4)           \
+  X(float, 4, 1, MODE_DIT, +1, 11, 1, 3, 512, 1, 1, 4)           \
   /* (three CTAs per SM, 80 registers: 58.6 us against 62.7 us at two) */ \
-  X(float, 4, 1, MODE_CONV, 0, 11, 0, 1, 256, 2, 1)
+  X(float, 4, 1, MODE_CONV, 0, 11, 0, 1, 256, 2, 1, 4)
 // Measured on C3 (2048^2): FP64 columns W=4 (32-byte rows) 53 us vs W=2
 // 68 us; FP32 columns W=8 34 us vs W=4 45 us -- row width, not occupancy,
 // bounds these passes (the narrower tiles were dropped from the list), and
 // neither do more warps: FP32 columns at 1024 threads per CTA (64 registers,
-// no spills) ran 30.0 / 30.6 us against 31.2 / 30.1 us.  On 3D 512 x 256 x 128 FP32 the specialised passes
+// no spills) ran 30.0 / 30.6 us against 31.2 / 30.1 us.  Radix-8 schedules
+// for 2048-point FP64 lines (RC = 3: fused pass at three 256-thread CTAs per
+// SM, 80 registers; columns at 1024 threads, 64 registers) ran 67 / 62 / 63
+// us against 54 / 47 / 51 us: the fourth stage's shared-memory round trip
+// costs more than the extra warps recover.  On 3D 512 x 256 x 128 FP32 the specialised passes
 // gain 4% over the generic kernel (256^3: 1%); specialising FP64 256-point
 // passes and the base-4 4096/16-point passes of 1D 2^16 measured 2-5%
 // slower than the generic kernel, so those shapes stay generic.
@@ -196,11 +202,11 @@ inline bool cluster_geometry(int bytes, int b2, int mode, int sign, int logL, in
 }
 
 inline bool special_geometry(int bytes, int b2, int mode, int sign, int logL, int cols, int tc,
-                             int* logW, int* nt, int variant = 0) {
+                             int rc, int* logW, int* nt, int variant = 0) {
   int seen = 0;
-#define PAC_X(T, BY, B2_, MO, SG, LL, CO, LW, NT_, MB, TC_)                               \
+#define PAC_X(T, BY, B2_, MO, SG, LL, CO, LW, NT_, MB, TC_, RC_)                          \
   if (bytes == BY && b2 == B2_ && mode == MO && (MO == MODE_CONV || sign == SG) &&     \
-      logL == LL && cols == CO && tc == TC_ && seen++ == variant) {                    \
+      logL == LL && cols == CO && tc == TC_ && rc == RC_ && seen++ == variant) {       \
     *logW = LW;                                                                        \
     *nt = NT_;                                                                         \
     return true;                                                                       \

@@ -779,14 +779,37 @@ PAC_HDC int sched_v(int lg, int b2, int i) {
   return (base + (i < extra ? 1 : 0)) * b2;
 }
 
-template <int LG, int B2, class IS>
+// The same rule with stages of at most RC bits (RC = 3: radix 8, fewer
+// registers per butterfly); RC >= 4 is sched_n / sched_v.
+PAC_HDC int sched_n_cap(int lg, int b2, int rc) {
+  if (b2 == 3 || rc >= 4) return sched_n(lg, b2);
+  const int per = rc / b2 > 0 ? rc / b2 : 1;  // digits per stage at most
+  return (lg / b2 + per - 1) / per;
+}
+PAC_HDC int sched_v_cap(int lg, int b2, int rc, int i) {
+  if (b2 == 3 || rc >= 4) return sched_v(lg, b2, i);
+  const int n = sched_n_cap(lg, b2, rc), digits = lg / b2;
+  return (digits / n + (i < digits % n ? 1 : 0)) * b2;
+}
+// does pass d run the RC-capped schedule of a 2^logL line?
+PAC_HD bool rads_match(const PassDesc& d, int logL, int b2, int rc) {
+  if (d.nst != sched_n_cap(logL, b2, rc)) return false;
+  for (int i = 0; i < d.nst; ++i)
+    if (d.rlog[i] != sched_v_cap(logL, b2, rc, i)) return false;
+  return true;
+}
+
+template <int LG, int B2, int RC, class IS>
 struct RadsImpl;
-template <int LG, int B2, int... I>
-struct RadsImpl<LG, B2, std::integer_sequence<int, I...>> {
-  using type = Rads<sched_v(LG, B2, I)...>;
+template <int LG, int B2, int RC, int... I>
+struct RadsImpl<LG, B2, RC, std::integer_sequence<int, I...>> {
+  using type = Rads<sched_v_cap(LG, B2, RC, I)...>;
 };
+template <int LG, int B2, int RC>
+using RadsCap =
+    typename RadsImpl<LG, B2, RC, std::make_integer_sequence<int, sched_n_cap(LG, B2, RC)>>::type;
 template <int LG, int B2>
-using RadsFor = typename RadsImpl<LG, B2, std::make_integer_sequence<int, sched_n(LG, B2)>>::type;
+using RadsFor = RadsCap<LG, B2, 4>;
 
 // shared-memory line pitch: one pad element every 16 (FP64) / 32 (FP32)
 // (FP32 8-line column tiles: sidx_col32), then skewed so that the W lines
