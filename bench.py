@@ -268,6 +268,12 @@ def run_ours(args, world, dist):
     x, h = make_inputs(args.config)
     x = x.reshape((batch,) + dims)
     h = h.reshape(dims)
+    if args.batch and args.batch != batch:
+        # --batch: the workload's signal repeated args.batch times in one plan
+        # (throughput of a batched plan; not the configuration's own line)
+        x = np.tile(x[:1], (args.batch,) + (1,) * len(dims))
+        batch = args.batch
+        cfg = dict(cfg, batch=batch)
 
     def t(a):
         return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
@@ -845,6 +851,9 @@ def main():
     ap.add_argument("--tune", choices=["on", "off"], default="on",
                     help="autotune the plan knobs (pac_autotune) before timing; the cache is "
                          "PAC_TUNE_CACHE if set, else a fresh file for this run")
+    ap.add_argument("--batch", type=int, default=0,
+                    help="override the configuration's batch (problems per plan); the "
+                         "signal is repeated")
     ap.add_argument("--knobs", default="",
                     help="explicit plan knobs for the timed plan, e.g. max_radix_log=3,w_shift=1 "
                          "(no tuning)")
