@@ -294,6 +294,11 @@ def run_ours(args, world, dist):
     tuned = tune_workload(L, args, dims, batch, form, sp)
     knobs = parse_knobs(args.knobs)
     l2_bytes = ybuf.numel() * ybuf.element_size() if args.l2 == "on" else 0
+    # only a window the L2 can hold: on 2048^2 FP64 the 64 MiB output window
+    # takes 27.1 -> 29.0 GElem/s at batch 1, while a 268 MB one (batch 4)
+    # thrashes (30.2 -> 19.3)
+    if l2_bytes > 0.75 * torch.cuda.get_device_properties(dev).L2_cache_size:
+        l2_bytes = 0
     if l2_bytes:
         pac.check(L, L.pac_stream_set_l2_persisting(sp, ybuf.data_ptr(), l2_bytes), "l2")
     # the tuned knobs (through PAC_TUNE_CACHE), or --knobs

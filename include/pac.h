@@ -324,7 +324,9 @@ PAC_API int pac_stream_wait_stream(pac_stream_t waiter, pac_stream_t waitee);
  * (CUDA access-policy window, persisting hits, streaming misses; the
  * persisting set-aside is a limit of this process's context only).
  * Meant for the convolution output, which the passes of pac_convolve use as
- * their intermediate.  bytes == 0 removes the window. */
+ * their intermediate, when it fits in L2: on 2048^2 FP64 a 64 MiB window
+ * gains 7%, while a window of several times the L2 (268 MB) made the same
+ * passes 36% slower than none.  bytes == 0 removes the window. */
 PAC_API int pac_stream_set_l2_persisting(pac_stream_t stream, const void* base, size_t bytes);
 
 /* Per-pass timing: while enabled, pac_convolve and pac_transform record a
