@@ -71,6 +71,8 @@ def _declare(L):
     L.pac_multi_autotune.argtypes = [i, C.POINTER(i), C.POINTER(i), i, i, _vp, C.c_char_p,
                                      C.POINTER(TuneResult)]
     L.pac_plan_destroy.argtypes = [_vp]
+    L.pac_plan_set_wait_limit.argtypes = [_vp, ll]
+    L.pac_plan_check_status.argtypes = [_vp, _vp]
     L.pac_filter_spectrum.argtypes = [_vp, _vp, _vp, i, _vp, _vp, d, _vp]
     L.pac_convolve.argtypes = [_vp, _vp, _vp, _vp, _vp, i, _vp, _vp, d, _vp]
     L.pac_spectrum_to_plan_order.argtypes = [_vp, _vp, _vp, i, _vp, _vp, d, _vp]

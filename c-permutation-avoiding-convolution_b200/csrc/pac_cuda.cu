@@ -26,6 +26,7 @@
 #include "pac.h"
 #include "pac_backend.h"
 #include "pac_special.h"
+#include "pac_tma.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -34,6 +35,10 @@ namespace pac {
 int set_error(int status, const char* fmt, ...);
 
 static std::atomic<long long> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+// the tensor-copy column passes (pac_coltma.cu)
+int launch_coltma(const PassDesc& d, int elem_bytes, int b2, long long grid, int threads,
+                  size_t smem, void* stream);
 
 static int cuda_fail(cudaError_t e, const char* what) {
   return set_error(PAC_ERROR_CUDA, "%s: %s", what, cudaGetErrorString(e));
@@ -178,57 +183,6 @@ __global__ void __launch_bounds__(NT, MINB) pac_cluster_kernel(const PassDesc d)
   if constexpr (MODE == MODE_DIT) cl.sync();
 }
 
-// ---------------------------------------------------------------------------
-// Tensor copies (TMA) and mbarriers for the pipelined column passes
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
-               : "memory");
-}
-__device__ __forceinline__ void fence_barrier_init() {
-  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-               "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-      " selp.u32 %0, 1, 0, p;\n}"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// bounded: gives up after ~2^31 SM cycles (about a second) instead of
-// spinning forever
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
-  const long long t0 = clock64();
-  while (!mbar_try_wait(bar, parity)) {
-    if (clock64() - t0 > (1LL << 31)) return false;
-  }
-  return true;
-}
-// box {W, BOXR, 1} of a 3D tensor map at (c0, c1, c2) into shared memory;
-// completion counted on bar.  No multicast.
-__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar,
-                                            int c0, int c1, int c2) {
-  asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
-      "l"((uint64_t)map), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
-      : "memory");
-}
-__device__ __forceinline__ void fence_proxy_async() {
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-
 // A pipelined column pass (ColPipe): persistent CTAs walk the tiles
 // blockIdx.x, blockIdx.x + gridDim.x, ...; thread 0 issues the tensor
 // copies of a CTA's next tile as soon as the current one is in registers.
@@ -271,10 +225,14 @@ __global__ void __launch_bounds__(NT, 1)
   Cx<T> x[CP::TPT];
   for (; tile < ntiles; tile += gridDim.x) {
     if (t < W) s_lb[t] = line_base(d, tile * W + t);
-    const bool ok = mbar_wait_bounded(&bar, phase);
+    const bool ok = mbar_wait_bounded(&bar, phase, wait_limit_of(d));
     if (!__syncthreads_and(ok)) {
-      if (t == 0 && d.status) atomicExch(d.status, PAC_ERROR_TIMEOUT);
-      if (!ok) mbar_wait_bounded(&bar, phase);  // copies still in flight
+      // a wait gave up: report it, issue nothing more, and keep the CTA (its
+      // shared memory) alive until the copies in flight have landed
+      if (t == 0) {
+        report_timeout(d);
+        mbar_wait_bounded(&bar, phase);
+      }
       break;
     }
     phase ^= 1;
@@ -821,21 +779,6 @@ int be_graph_destroy(void* exec) {
   return PAC_SUCCESS;
 }
 
-// cuTensorMapEncodeTiled through the runtime's driver entry point (no -lcuda)
-static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-  static std::once_flag once;
-  std::call_once(once, [] {
-    void* p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
-            cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
-  });
-  return fn;
-}
-
 // 3D view (S columns, L rows, O = nlines / S outer) of a column pass's input
 // array; box W x boxr x 1, unswizzled, so a box lands as dense rows of W
 // elements
@@ -893,6 +836,7 @@ static int launch_pipe(const PassDesc& d, int elem_bytes, int b2, long long grid
 
 int be_launch_pass(const PassDesc& d, int elem_bytes, int b2, long long grid, int threads,
                    size_t smem, void* stream) {
+  if (d.tma) return launch_coltma(d, elem_bytes, b2, grid, threads, smem, stream);
   if (d.pipe) return launch_pipe(d, elem_bytes, b2, grid, threads, smem, stream);
   if (d.logC > 0) return launch_cluster(d, elem_bytes, b2, grid, threads, smem, stream);
   if (d.spec) {

@@ -14,7 +14,9 @@
  * Errors: the reference functions return void and do not validate.  Here an
  * axis length that is not a power of r, a NULL array or a CUDA failure
  * leaves the caller's data untouched, prints one line to stderr and records
- * the status for pac_get_last_status().
+ * the status for pac_get_last_status().  A device wait that gave up during
+ * the call (pac_plan_check_status) is reported the same way, as
+ * PAC_ERROR_TIMEOUT; the outputs of that call are then incomplete.
  */
 #include <math.h>
 #include <pthread.h>
@@ -76,8 +78,16 @@ static int check_dims(int rank, const int* dims, int r, const char* fn) {
 /* ------------------------------------------------------------------------ */
 #define CACHE_SLOTS 16
 
+/* An entry is pinned (pins > 0) from the moment a caller picks it under the
+ * cache lock until it releases it; eviction only ever takes unpinned
+ * entries, so an entry cannot be refilled with another shape between the
+ * caller's lookup and its use.  When every slot is pinned (more concurrent
+ * callers on distinct shapes than slots) the caller gets a private entry
+ * that is freed on release. */
 typedef struct {
   int used;
+  int pins;        /* callers holding or waiting for this entry (cache lock) */
+  int temporary;   /* private entry outside the cache, freed on release */
   int rank, dims[3], r;
   long long N;
   pac_plan_t plan; /* NULL for shapes the butterflies do not run on */
@@ -111,6 +121,25 @@ static void entry_release(entry_t* e) {
   e->used = 0;
 }
 
+/* plan, staging buffers and streams of an entry for (rank, dims, r) */
+static int entry_fill(entry_t* e, int rank, const int* dims, int r, int want_plan) {
+  e->used = 1;
+  e->rank = rank;
+  e->r = r;
+  e->N = 1;
+  for (int a = 0; a < 3; ++a) e->dims[a] = a < rank ? dims[a] : 1;
+  for (int a = 0; a < rank; ++a) e->N *= dims[a];
+  int st = PAC_SUCCESS;
+  if (want_plan) st = pac_plan_create(&e->plan, rank, dims, 1, r, PAC_FORM_F64);
+  if (st == PAC_SUCCESS) st = pac_malloc((void**)&e->x, (size_t)e->N * 16);
+  if (st == PAC_SUCCESS) st = pac_malloc((void**)&e->h, (size_t)e->N * 16);
+  if (st == PAC_SUCCESS) st = pac_malloc((void**)&e->rho, (size_t)e->N * sizeof(int));
+  if (st == PAC_SUCCESS) st = pac_stream_create(&e->s1);
+  if (st == PAC_SUCCESS) st = pac_stream_create(&e->s2);
+  if (st != PAC_SUCCESS) entry_release(e);
+  return st;
+}
+
 /* Returns a locked entry for (rank, dims, r); want_plan selects whether the
  * butterfly plan is built (radix supported and dims valid). */
 static int acquire(int rank, const int* dims, int r, int want_plan, entry_t** out) {
@@ -124,50 +153,72 @@ static int acquire(int rank, const int* dims, int r, int want_plan, entry_t** ou
     for (int a = 0; a < rank; ++a) same &= e->dims[a] == dims[a];
     if (same) hit = e;
   }
-  if (!hit) {
-    /* free slot, else evict the least recently used one */
-    entry_t* victim = NULL;
-    for (int i = 0; i < CACHE_SLOTS && !victim; ++i)
-      if (!g_cache[i].used) victim = &g_cache[i];
-    if (!victim) {
-      victim = &g_cache[0];
-      for (int i = 1; i < CACHE_SLOTS; ++i)
-        if (g_cache[i].last_use < victim->last_use) victim = &g_cache[i];
-    }
-    pthread_mutex_lock(&victim->mu);
-    if (victim->used) entry_release(victim);
-    victim->used = 1;
-    victim->rank = rank;
-    victim->r = r;
-    victim->N = 1;
-    for (int a = 0; a < 3; ++a) victim->dims[a] = a < rank ? dims[a] : 1;
-    for (int a = 0; a < rank; ++a) victim->N *= dims[a];
-    int st = PAC_SUCCESS;
-    if (want_plan) st = pac_plan_create(&victim->plan, rank, dims, 1, r, PAC_FORM_F64);
-    if (st == PAC_SUCCESS) st = pac_malloc((void**)&victim->x, (size_t)victim->N * 16);
-    if (st == PAC_SUCCESS) st = pac_malloc((void**)&victim->h, (size_t)victim->N * 16);
-    if (st == PAC_SUCCESS) st = pac_malloc((void**)&victim->rho, (size_t)victim->N * sizeof(int));
-    if (st == PAC_SUCCESS) st = pac_stream_create(&victim->s1);
-    if (st == PAC_SUCCESS) st = pac_stream_create(&victim->s2);
-    if (st != PAC_SUCCESS) {
-      entry_release(victim);
-      pthread_mutex_unlock(&victim->mu);
-      pthread_mutex_unlock(&g_cache_mu);
-      return st;
-    }
-    victim->last_use = ++g_tick;
+  if (hit) {
+    hit->pins++;
+    hit->last_use = ++g_tick;
     pthread_mutex_unlock(&g_cache_mu);
-    *out = victim;
+    pthread_mutex_lock(&hit->mu);  /* pinned: still this shape once locked */
+    *out = hit;
     return PAC_SUCCESS;
   }
-  hit->last_use = ++g_tick;
+  /* free slot, else evict the least recently used unpinned one */
+  entry_t* victim = NULL;
+  for (int i = 0; i < CACHE_SLOTS && !victim; ++i)
+    if (!g_cache[i].used && !g_cache[i].pins) victim = &g_cache[i];
+  if (!victim) {
+    for (int i = 0; i < CACHE_SLOTS; ++i) {
+      entry_t* e = &g_cache[i];
+      if (e->pins) continue;
+      if (!victim || e->last_use < victim->last_use) victim = e;
+    }
+  }
+  if (!victim) {
+    /* every slot is in use by another caller: a private entry */
+    pthread_mutex_unlock(&g_cache_mu);
+    entry_t* e = (entry_t*)calloc(1, sizeof(entry_t));
+    if (!e) return PAC_ERROR_ALLOC;
+    pthread_mutex_init(&e->mu, NULL);
+    e->temporary = 1;
+    e->pins = 1;
+    int st = entry_fill(e, rank, dims, r, want_plan);
+    if (st != PAC_SUCCESS) {
+      pthread_mutex_destroy(&e->mu);
+      free(e);
+      return st;
+    }
+    pthread_mutex_lock(&e->mu);
+    *out = e;
+    return PAC_SUCCESS;
+  }
+  /* unpinned: no caller holds its lock or waits for it */
+  victim->pins++;
+  pthread_mutex_lock(&victim->mu);
+  if (victim->used) entry_release(victim);
+  int st = entry_fill(victim, rank, dims, r, want_plan);
+  if (st != PAC_SUCCESS) {
+    victim->pins--;
+    pthread_mutex_unlock(&victim->mu);
+    pthread_mutex_unlock(&g_cache_mu);
+    return st;
+  }
+  victim->last_use = ++g_tick;
   pthread_mutex_unlock(&g_cache_mu);
-  pthread_mutex_lock(&hit->mu);
-  *out = hit;
+  *out = victim;
   return PAC_SUCCESS;
 }
 
-static void release(entry_t* e) { pthread_mutex_unlock(&e->mu); }
+static void release(entry_t* e) {
+  pthread_mutex_unlock(&e->mu);
+  if (e->temporary) {
+    entry_release(e);
+    pthread_mutex_destroy(&e->mu);
+    free(e);
+    return;
+  }
+  pthread_mutex_lock(&g_cache_mu);
+  e->pins--;
+  pthread_mutex_unlock(&g_cache_mu);
+}
 
 #define TRY(x)                  \
   do {                          \
@@ -222,6 +273,7 @@ static void run_op(const char* fn, int rank, const int* dims, int r, int kind, i
   TRY(pac_memcpy_d2h(re, xr, nb, e->s1));
   TRY(pac_memcpy_d2h(im, xi, nb, e->s1));
   TRY(pac_stream_synchronize(e->s1));
+  if (e->plan) TRY(pac_plan_check_status(e->plan, e->s1));
 done:
   release(e);
   report(st, fn);
@@ -278,6 +330,7 @@ static void run_pac_conv(const char* fn, int rank, const int* dims, int r, doubl
   TRY(pac_memcpy_d2h(im, xi, nb, e->s2));
   TRY(pac_stream_synchronize(e->s1));
   TRY(pac_stream_synchronize(e->s2));
+  if (e->plan) TRY(pac_plan_check_status(e->plan, e->s1));
 done:
   release(e);
   report(st, fn);
@@ -327,6 +380,7 @@ static void run_fft_conv(const char* fn, int rank, const int* dims, int r, doubl
   TRY(pac_memcpy_d2h(re, xr, nb, e->s1));
   TRY(pac_memcpy_d2h(im, xi, nb, e->s1));
   TRY(pac_stream_synchronize(e->s1));
+  if (e->plan) TRY(pac_plan_check_status(e->plan, e->s1));
 done:
   release(e);
   report(st, fn);

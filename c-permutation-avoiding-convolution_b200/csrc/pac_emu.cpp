@@ -113,6 +113,17 @@ static void replay_special(const PassDesc& d, long long grid) {
   }
 }
 
+// The replay models a tensor copy as landing kCopyCycles SM cycles after it
+// is issued: a pass whose wait limit is below that gives up on its first
+// tile in every CTA, as on the device -- it reports PAC_ERROR_TIMEOUT in the
+// plan's status word and writes no output.
+static const long long kCopyCycles = 1000;
+static bool copy_wait_gives_up(const PassDesc& d) {
+  if (d.wait_limit <= 0 || d.wait_limit >= kCopyCycles) return false;
+  if (d.status) *d.status = PAC_ERROR_TIMEOUT;
+  return true;
+}
+
 // replay of a pipelined column kernel: the CTAs of the persistent launch
 // visit their tiles in order; the tensor copy becomes a plain copy of the
 // tile into the dense buffer, and each step between two barriers runs for
@@ -122,6 +133,7 @@ template <typename T, int B2, int MODE, int SIGN, int LOGL, int LOGW, int NT>
 static void replay_pipe(const PassDesc& d, long long grid) {
   using CP = ColPipe<T, B2, MODE, SIGN, LOGL, LOGW, NT>;
   constexpr int W = CP::W, L = CP::L, NS = CP::NS;
+  if (copy_wait_gives_up(d)) return;
   struct Regs {
     Cx<T> v[CP::TPT];
   };
@@ -195,8 +207,114 @@ static void replay_cluster(const PassDesc& d, long long grid) {
   }
 }
 
+// replay of a tensor-copy column kernel (ColTma): the CTAs of the
+// persistent launch visit their tiles in order; the tensor load and store
+// become plain copies through the same layout maps (dense rows or the
+// transposed view), and every step runs its reads, its arithmetic and its
+// writes for all threads in turn -- the order the kernel's barriers impose.
+// The buffer starts every tile as NaN, so a read of a slot that no copy or
+// stage wrote shows up in the results.
+template <typename T, int B2, int MODE, int SIGN, int LOGL, int LOGW, int NT, int PIPE>
+static int replay_coltma(const PassDesc& d, long long grid) {
+  using CT = ColTma<T, B2, MODE, SIGN, LOGL, LOGW, NT>;
+  constexpr int W = CT::W, L = CT::L, NS = CT::NS, TILE = CT::TILE;
+  if (copy_wait_gives_up(d)) return PAC_SUCCESS;
+  struct Regs {
+    Cx<T> v[CT::TPT];
+  };
+  std::vector<T> B((size_t)2 * TILE);
+  std::vector<Regs> xs(NT);
+  T* Bre = B.data();
+  T* Bim = B.data() + TILE;
+  const T* ire = (const T*)d.in_re;
+  const T* iim = (const T*)d.in_im;
+  T* ore = (T*)d.out_re;
+  T* oim = (T*)d.out_im;
+  const long long S = 1LL << d.logS;
+  const long long ntiles = d.nlines >> LOGW;
+  auto each = [&](auto&& f) {
+    for (int t = 0; t < NT; ++t) f(t, xs[t].v);
+  };
+  // every layout map is a bijection of the tile onto [0, TILE)
+  {
+    std::vector<char> seen(3 * TILE, 0);
+    for (int e = 0; e < L; ++e)
+      for (int w = 0; w < W; ++w) {
+        const int q[3] = {CT::template pos<LAY_DENSE>(e, w), CT::template pos<LAY_TRANS>(e, w),
+                          CT::template pos<LAY_SWZ>(e, w)};
+        for (int k = 0; k < 3; ++k) {
+          if (q[k] < 0 || q[k] >= TILE || seen[k * TILE + q[k]]++)
+            return set_error(PAC_ERROR_INTERNAL, "tensor-copy layout %d is not a bijection", k);
+        }
+      }
+  }
+  if (d.nlines % W || (1LL << d.logS) % W)
+    return set_error(PAC_ERROR_INTERNAL, "tensor-copy tiles do not cover the lines");
+  for (long long c = 0; c < grid; ++c)
+    for (long long tile = c; tile < ntiles; tile += grid) {
+      int i0, o;
+      CT::tile_coords(d, tile, i0, o);
+      const long long base = (long long)o * L * S + i0;
+      std::fill(B.begin(), B.end(), std::numeric_limits<T>::quiet_NaN());
+      for (int e = 0; e < L; ++e)
+        for (int w = 0; w < W; ++w) {
+          const int q = CT::DIF ? CT::template pos<LAY_DENSE>(e, w)
+                                : CT::template pos<LAY_TRANS>(e, w);
+          Bre[q] = ire[base + e * S + w];
+          Bim[q] = iim[base + e * S + w];
+        }
+      if constexpr (PIPE) {
+        // registers between the steps, one-component exchanges through X,
+        // the result written into X component by component for the stores
+        constexpr int LOUT = CT::DIF ? LAY_TRANS : LAY_DENSE;
+        std::vector<T> X((size_t)TILE, std::numeric_limits<T>::quiet_NaN());
+        each([&](int t, Cx<T>(&x)[CT::TPT]) { CT::template read<0>(t, Bre, Bim, x); });
+        std::fill(B.begin(), B.end(), std::numeric_limits<T>::quiet_NaN());
+        static_for<NS>([&](auto ss) {
+          constexpr int St = ss.value;
+          each([&](int t, Cx<T>(&x)[CT::TPT]) { CT::template compute<St>(d, tile, t, x); });
+          if constexpr (St < NS - 1) {
+            each([&](int t, Cx<T>(&x)[CT::TPT]) { CT::template write_c<St, 0, LAY_SWZ>(d, t, X.data(), x); });
+            each([&](int t, Cx<T>(&x)[CT::TPT]) { CT::template read_c<St + 1, 0, LAY_SWZ>(t, X.data(), x); });
+            each([&](int t, Cx<T>(&x)[CT::TPT]) { CT::template write_c<St, 1, LAY_SWZ>(d, t, X.data(), x); });
+            each([&](int t, Cx<T>(&x)[CT::TPT]) { CT::template read_c<St + 1, 1, LAY_SWZ>(t, X.data(), x); });
+          }
+        });
+        each([&](int t, Cx<T>(&x)[CT::TPT]) { CT::template write_c<NS - 1, 0, LOUT>(d, t, Bre, x); });
+        each([&](int t, Cx<T>(&x)[CT::TPT]) { CT::template write_c<NS - 1, 1, LOUT>(d, t, Bim, x); });
+      } else {
+        static_for<NS>([&](auto ss) {
+          constexpr int St = ss.value;
+          each([&](int t, Cx<T>(&x)[CT::TPT]) { CT::template read<St>(t, Bre, Bim, x); });
+          each([&](int t, Cx<T>(&x)[CT::TPT]) { CT::template compute<St>(d, tile, t, x); });
+          each([&](int t, Cx<T>(&x)[CT::TPT]) { CT::template write<St>(d, t, Bre, Bim, x); });
+        });
+      }
+      for (int e = 0; e < L; ++e)
+        for (int w = 0; w < W; ++w) {
+          const int q = CT::DIF ? CT::template pos<LAY_TRANS>(e, w)
+                                : CT::template pos<LAY_DENSE>(e, w);
+          ore[base + e * S + w] = Bre[q];
+          oim[base + e * S + w] = Bim[q];
+        }
+    }
+  return PAC_SUCCESS;
+}
+
 int be_launch_pass(const PassDesc& d, int elem_bytes, int b2, long long grid, int threads,
                    size_t, void*) {
+  if (d.tma) {
+    int seen = 0;  // candidates of this geometry so far; d.tma - 1 picks one
+#define PAC_X(T, BY, B2_, MO, SG, LL, LW, NT_, MB, PP, DF)                                      \
+  if (elem_bytes == BY && b2 == B2_ && d.mode == MO && d.sign == SG && d.logL == LL &&     \
+      seen++ == d.tma - 1 && d.W == (1 << LW) && threads == NT_) {                         \
+    g_launches++;                                                                          \
+    return replay_coltma<T, B2_, MO, SG, LL, LW, NT_, PP>(d, grid);                        \
+  }
+    PAC_COLTMA_LIST(PAC_X)
+#undef PAC_X
+    return set_error(PAC_ERROR_INTERNAL, "no tensor-copy replay for a pass marked so");
+  }
   if (d.pipe) {
 #define PAC_X(T, BY, B2_, MO, SG, LL, LW, NT_)                                               \
   if (elem_bytes == BY && b2 == B2_ && d.mode == MO && d.sign == SG && d.logL == LL &&      \

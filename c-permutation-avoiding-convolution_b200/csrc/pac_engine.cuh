@@ -83,8 +83,12 @@ struct PassDesc {
   int nat_nf;
   int nat_flog[PAC_MAX_FACTORS];
   int nat_Mlog;
-  // device status word (bounded waits report here); may be null
+  // device status word of the plan: a bounded wait that gives up writes
+  // PAC_ERROR_TIMEOUT here; may be null
   int* status;
+  // spin limit of the pass's bounded waits, in SM clock cycles (<= 0: the
+  // default, 2^31 cycles, about a second)
+  long long wait_limit;
   // 1: this pass runs the kernel specialised for its geometry (pac_special.h)
   int spec;
   // > 0: a cluster of 2^logC CTAs shares each tile of this specialised
@@ -93,6 +97,9 @@ struct PassDesc {
   // 1: pipelined column pass, one persistent CTA per SM with tensor-copy
   // prefetch of the next tile (pac_special.h, PAC_PIPE_LIST; ColPipe)
   int pipe;
+  // k > 0: column pass staged through shared memory by tensor copies, the
+  // k-th geometry of its kind on PAC_COLTMA_LIST (pac_special.h; ColTma)
+  int tma;
   // 1: tensor-core form, radix-16 stages on the tensor cores (pac_tc.cuh);
   // tcc: their DFT operands, per stage kind and lane (tc_const_set)
   int tc;
@@ -340,3 +347,4 @@ PAC_HD void nat_line(const PassDesc& d, long long g, long long* in_base, long lo
 
 }  // namespace pac
 #include "pac_stages.cuh"
+#include "pac_coltma.cuh"

@@ -64,16 +64,17 @@ extern "C" PAC_API int pac_convolve_1d_noalloc(const double* x_re, const double*
                                                pac_stream_t stream) {
   if (!x_re || !x_im || !h_re || !h_im || !y_re || !y_im || batch < 1)
     return pac::set_error(PAC_ERROR_INVALID_VALUE, "pac_convolve_1d_noalloc: bad argument");
-  int logn = 0;
-  while (logn < 31 && (1 << logn) < n) ++logn;
-  if (n < 1 || (1 << logn) != n)
-    return pac::set_error(PAC_ERROR_NOT_POWER,
-                          "pac_convolve_1d_noalloc: n = %d is not a power of 2", n);
+  // the size limit first: it bounds every shift below
   if (n > PAC_NOALLOC_MAX_N)
     return pac::set_error(PAC_ERROR_SIZE,
                           "pac_convolve_1d_noalloc: n = %d exceeds the no-allocation limit %d "
                           "(its scratch is a fixed %d-byte static device array)",
                           n, PAC_NOALLOC_MAX_N, PAC_NOALLOC_SCRATCH_BYTES);
+  if (n < 1 || (n & (n - 1)) != 0)
+    return pac::set_error(PAC_ERROR_NOT_POWER,
+                          "pac_convolve_1d_noalloc: n = %d is not a power of 2", n);
+  int logn = 0;
+  while ((1 << logn) < n) ++logn;
   int st = pac::be_init();
   if (st != PAC_SUCCESS) return st;
   void* scratch = nullptr;

@@ -130,7 +130,29 @@ static int max_factor_log(int bytes, int b2, int cap = 0) {
   return lmax - lmax % b2;
 }
 
-static int build_schedule(Schedule& s, int rank, const int* logs, const int* b2s, int bytes) {
+// Device memory for a schedule's tables: cudaMalloc'd (freed by the
+// Schedule), or carved out of caller-supplied scratch (Arena; nothing to
+// free).
+struct Arena {
+  char* cur;
+  char* end;
+  void* take(size_t bytes) {
+    size_t a = (bytes + 255) & ~(size_t)255;
+    if (cur + a > end) return nullptr;
+    void* p = cur;
+    cur += a;
+    return p;
+  }
+};
+static int table_alloc(Arena* ar, void** p, size_t bytes) {
+  if (!ar) return be_malloc(p, bytes);
+  *p = ar->take(bytes);
+  return *p ? PAC_SUCCESS : set_error(PAC_ERROR_SIZE, "no-allocation scratch too small");
+}
+
+// The factors of every axis and their stage radices -- the one rule every
+// plan follows (allocating plans and the no-allocation entry point alike).
+static int split_axes(Schedule& s, int rank, const int* logs, const int* b2s, int bytes) {
   s.bytes = bytes;
   s.b2 = b2s[rank - 1];
   for (int a = 0; a < rank; ++a) {
@@ -160,7 +182,13 @@ static int build_schedule(Schedule& s, int rank, const int* logs, const int* b2s
                        "a factor of 2^%d needs %zu stages of radix <= 2^%d (at most %d)", v.log,
                        s.rad.back().size(), s.rlog_cap, (int)PAC_MAX_STAGES);
   }
-  // stage twiddle tables
+  return PAC_SUCCESS;
+}
+
+// Stage and 4-step twiddle tables of a split schedule, in memory from
+// table_alloc, generated on `stream`.
+static int build_tables(Schedule& s, Arena* ar, void* stream) {
+  const int bytes = s.bytes;
   std::vector<std::pair<int, int>> specs;
   long long total = 0;
   for (size_t i = 0; i < s.vax.size(); ++i) {
@@ -176,10 +204,10 @@ static int build_schedule(Schedule& s, int rank, const int* logs, const int* b2s
     }
   }
   if (total > 0) {
-    PAC_TRY(be_malloc(&s.pool, (size_t)total * 2 * bytes));
+    PAC_TRY(table_alloc(ar, &s.pool, (size_t)total * 2 * bytes));
     for (auto& k : specs) {
       char* dst = (char*)s.pool + (size_t)s.tw_off[k] * 2 * bytes;
-      PAC_TRY(be_fill_stage_tw(dst, bytes, k.first, k.second, nullptr));
+      PAC_TRY(be_fill_stage_tw(dst, bytes, k.first, k.second, stream));
     }
   }
   // 4-step twiddles: for every non-last factor, N = L * (later factors of its axis)
@@ -191,12 +219,22 @@ static int build_schedule(Schedule& s, int rank, const int* logs, const int* b2s
     Schedule::Tw4 t;
     t.lolog = (logN + 1) / 2;
     long long nlo = 1LL << t.lolog, nhi = 1LL << (logN - t.lolog);
-    PAC_TRY(be_malloc(&t.lo, (size_t)nlo * 2 * bytes));
-    PAC_TRY(be_malloc(&t.hi, (size_t)nhi * 2 * bytes));
-    PAC_TRY(be_fill_pow_tw(t.lo, bytes, nlo, 1, logN, nullptr));
-    PAC_TRY(be_fill_pow_tw(t.hi, bytes, nhi, nlo, logN, nullptr));
+    PAC_TRY(table_alloc(ar, &t.lo, (size_t)nlo * 2 * bytes));
+    int st = table_alloc(ar, &t.hi, (size_t)nhi * 2 * bytes);
+    if (st != PAC_SUCCESS) {
+      if (!ar) be_free(t.lo);
+      return st;
+    }
     s.tw4[logN] = t;
+    PAC_TRY(be_fill_pow_tw(t.lo, bytes, nlo, 1, logN, stream));
+    PAC_TRY(be_fill_pow_tw(t.hi, bytes, nhi, nlo, logN, stream));
   }
+  return PAC_SUCCESS;
+}
+
+static int build_schedule(Schedule& s, int rank, const int* logs, const int* b2s, int bytes) {
+  PAC_TRY(split_axes(s, rank, logs, b2s, bytes));
+  PAC_TRY(build_tables(s, nullptr, nullptr));
   // the tables are filled on the legacy stream, which does not order against
   // non-blocking streams: finish them before the plan is handed out
   return be_stream_sync(nullptr);
@@ -224,6 +262,10 @@ struct pac_plan_s {
   size_t ws_bytes = 0;
   void* tmp64 = nullptr;  // FP64 temporary for the F32 filter spectrum
   size_t tmp64_bytes = 0;
+  // device status word of the bounded waits (pac_plan_check_status) and
+  // their spin limit in SM cycles (0: the kernels' default)
+  int* status = nullptr;
+  long long wait_limit = 0;
   // per-pass timing (pac_plan_set_pass_timing)
   int timing = 0;
   std::mutex t_mu;
@@ -233,6 +275,7 @@ struct pac_plan_s {
   ~pac_plan_s() {
     if (ws) pac::be_free(ws);
     if (tmp64) pac::be_free(tmp64);
+    if (status) pac::be_free(status);
     for (void* e : t_ev) pac::be_event_destroy(e);
   }
 };
@@ -375,6 +418,33 @@ static void apply_special(const Schedule& s, PassSpec& p) {
     p.smem = (size_t)2 * d.W * d.L * s.bytes + (size_t)d.W * d.pitch * s.bytes + 1024;
     return;
   }
+  // column pass staged by tensor copies: PAC_COLTMA=k picks the k-th
+  // candidate of its geometry, 0 none; unset, the geometry's default entry.
+  // Plain DIF / DIT passes of the default radix schedule, 16-byte aligned
+  // arrays; not with specialised kernels tuned off.
+  const char* tv = getenv("PAC_COLTMA");
+  const int tvar = (d.tc || s.rlog_cap < 4 || s.special < 0) ? 0 : tv ? atoi(tv) : -1;
+  int tminb = 1, tpipe = 0, tcand = 0;
+  if (d.logS > 0 && cvar == nullptr && tvar != 0 && d.tw4 == 0 &&
+      (d.mode == MODE_DIF || d.mode == MODE_DIT) &&
+      coltma_geometry(s.bytes, p.b2, d.mode, d.sign, d.logL, &logW, &nt, &tminb, &tpipe,
+                      tvar > 0 ? tvar - 1 : -1, &tcand) &&
+      rads_match(d, d.logL, p.b2, 4) && logW <= d.logS &&
+      (d.nlines & ((1LL << logW) - 1)) == 0 && (d.nlines >> d.logS) < (1LL << 31) &&
+      ((uintptr_t)d.in_re | (uintptr_t)d.in_im | (uintptr_t)d.out_re | (uintptr_t)d.out_im) %
+              16 == 0) {
+    d.W = 1 << logW;
+    d.logW = logW;
+    d.nthreads = nt;
+    d.spec = 1;
+    d.tma = tcand;
+    const long long tiles = d.nlines >> logW;
+    const long long slots = (long long)be_num_sms() * tminb;
+    p.threads = nt;
+    p.grid = tiles < slots ? tiles : slots;
+    p.smem = (size_t)(tpipe ? 3 : 2) * d.W * d.L * s.bytes + 1024;
+    return;
+  }
   const char* var = getenv("PAC_SPECIAL_VARIANT");
   int variant = s.special > 0 ? s.special : var ? atoi(var) : 0;
   const int cols = d.logS > 0 ? 1 : 0;
@@ -436,7 +506,11 @@ static int launch(const Schedule& s, PassSpec& p, void* stream) {
 // events and accumulate the per-pass milliseconds in the plan.
 static int exec_passes(pac_plan_s* pl, const Schedule& s, std::vector<PassSpec>& passes,
                        void* stream) {
-  for (auto& p : passes) apply_special(s, p);
+  for (auto& p : passes) {
+    p.d.status = pl->status;
+    p.d.wait_limit = pl->wait_limit;
+    apply_special(s, p);
+  }
   if (!pl->timing) {
     for (auto& p : passes) PAC_TRY(launch(s, p, stream));
     return PAC_SUCCESS;
@@ -681,67 +755,10 @@ static int to_plan_order(pac_plan_s* pl, const double* in_re, const double* in_i
 // call never depends on what an earlier call left there.  Nothing here
 // allocates device memory.
 // ---------------------------------------------------------------------------
-struct Arena {
-  char* cur;
-  char* end;
-  void* take(size_t bytes) {
-    size_t a = (bytes + 255) & ~(size_t)255;
-    if (cur + a > end) return nullptr;
-    void* p = cur;
-    cur += a;
-    return p;
-  }
-};
-
 static int build_schedule_in_arena(Schedule& s, int logn, Arena& ar, void* stream) {
-  s.bytes = 8;
-  s.b2 = 1;
-  const int lmax = max_factor_log(8, 1);
-  if (logn > 0) {
-    int nf = (logn + lmax - 1) / lmax;
-    if (nf > PAC_MAX_FACTORS) return set_error(PAC_ERROR_SIZE, "too many factors");
-    std::vector<int> parts(nf, logn / nf);
-    for (int i = 0; i < logn % nf; ++i) parts[nf - 1 - i]++;
-    for (int f = 0; f < nf; ++f) s.vax.push_back({parts[f], 0, f == 0, f == nf - 1, 1});
-  }
-  for (auto& v : s.vax) s.rad.push_back(radix_schedule(v.log, 1));
-  long long total = 0;
-  std::vector<std::pair<int, int>> specs;
-  for (size_t i = 0; i < s.vax.size(); ++i) {
-    int logK = s.vax[i].log;
-    for (int rl : s.rad[i]) {
-      std::pair<int, int> key(logK, rl);
-      if (!s.tw_off.count(key) && logK > rl) {
-        s.tw_off[key] = (int)total;
-        specs.push_back(key);
-        total += (1LL << (logK - rl)) * ((1LL << rl) - 1);
-      }
-      logK -= rl;
-    }
-  }
-  if (total > 0) {
-    s.pool = ar.take((size_t)total * 16);
-    if (!s.pool) return set_error(PAC_ERROR_SIZE, "no-allocation scratch too small");
-    for (auto& k : specs)
-      PAC_TRY(be_fill_stage_tw((char*)s.pool + (size_t)s.tw_off[k] * 16, 8, k.first, k.second,
-                               stream));
-  }
-  for (size_t i = 0; i < s.vax.size(); ++i) {
-    if (s.vax[i].last) continue;
-    int logN = 0;
-    for (size_t j = i; j < s.vax.size(); ++j) logN += s.vax[j].log;
-    if (s.tw4.count(logN)) continue;
-    Schedule::Tw4 t;
-    t.lolog = (logN + 1) / 2;
-    long long nlo = 1LL << t.lolog, nhi = 1LL << (logN - t.lolog);
-    t.lo = ar.take((size_t)nlo * 16);
-    t.hi = ar.take((size_t)nhi * 16);
-    if (!t.lo || !t.hi) return set_error(PAC_ERROR_SIZE, "no-allocation scratch too small");
-    s.tw4[logN] = t;
-    PAC_TRY(be_fill_pow_tw(t.lo, 8, nlo, 1, logN, stream));
-    PAC_TRY(be_fill_pow_tw(t.hi, 8, nhi, nlo, logN, stream));
-  }
-  return PAC_SUCCESS;
+  const int logs[1] = {logn}, b2s[1] = {1};
+  if (logn > 0) PAC_TRY(split_axes(s, 1, logs, b2s, 8));
+  return build_tables(s, &ar, stream);
 }
 
 int conv_in_scratch(void* scratch, size_t scratch_bytes, int logn, int batch, const double* x_re,
@@ -857,6 +874,10 @@ static int create_plan(pac_plan_t* plan, int rank, const int* dims, const int* d
     st = build_schedule(*p->s64, rank, p->logs, b2s, 8);
     if (st != PAC_SUCCESS) return st;
   }
+  st = be_malloc((void**)&p->status, sizeof(int));
+  if (st == PAC_SUCCESS) st = be_memset(p->status, 0, sizeof(int), nullptr);
+  if (st == PAC_SUCCESS) st = be_stream_sync(nullptr);
+  if (st != PAC_SUCCESS) return st;
   *plan = p.release();
   return PAC_SUCCESS;
 }
@@ -1075,6 +1096,25 @@ PAC_API int pac_plan_get_pass_timing(pac_plan_t plan, int max_passes, double* ms
   std::fill(plan->t_ms.begin(), plan->t_ms.end(), 0.0);
   plan->t_calls = 0;
   return PAC_SUCCESS;
+}
+
+PAC_API int pac_plan_set_wait_limit(pac_plan_t plan, long long cycles) {
+  if (!plan) return set_error(PAC_ERROR_INVALID_VALUE, "pac_plan_set_wait_limit: NULL plan");
+  plan->wait_limit = cycles > 0 ? cycles : 0;
+  return PAC_SUCCESS;
+}
+
+PAC_API int pac_plan_check_status(pac_plan_t plan, pac_stream_t stream) {
+  if (!plan) return set_error(PAC_ERROR_INVALID_VALUE, "pac_plan_check_status: NULL plan");
+  int word = 0;
+  PAC_TRY(be_stream_sync(stream));
+  PAC_TRY(be_memcpy(&word, plan->status, sizeof(int), CPY_D2H, stream));
+  PAC_TRY(be_stream_sync(stream));
+  if (word == PAC_SUCCESS) return PAC_SUCCESS;
+  PAC_TRY(be_memset(plan->status, 0, sizeof(int), stream));
+  PAC_TRY(be_stream_sync(stream));
+  return set_error(word, "a bounded device wait of this plan gave up (status %d); the output "
+                         "of the call it belongs to is incomplete", word);
 }
 
 PAC_API const char* pac_status_string(int status) {

@@ -120,6 +120,56 @@ namespace pac {
   X(float, 4, 1, MODE_DIF, -1, 11, 3, 512)          \
   X(float, 4, 1, MODE_DIT, +1, 11, 3, 512)
 
+// Column passes staged by tensor copies (PassDesc.tma, ColTma in
+// pac_coltma.cuh): persistent CTAs, the tile moved between global and shared
+// memory by tensor copies in both directions, conflict-free layouts in
+// shared memory.  PIPE = 1: the pipelined variant (tile in registers, the
+// next tile's tensor load in flight meanwhile, exchanges through a
+// one-component buffer).  For each geometry the first entry is candidate 1,
+// the next candidate 2, ... (PassDesc.tma = candidate); PAC_COLTMA=k picks
+// the k-th, 0 none, and without it a geometry runs its DEF = 1 entry.
+// Measured on 2048^2 (per DIF / DIT pass): FP64 one-CTA tiles 61.8 / 55.5 us,
+// W = 2 at two CTAs per SM 62.0 / 54.0, pipelined 53.1 / 47.6, against
+// 54.9 / 51.0 for the load/store-unit kernel (pac_special.h above): the
+// pipelined FP64 variant is the default.  FP32: 36.8 / 32.8, 41.2 / 34.8
+// and 47.4 / 36.9 (the pipelined FP32 tile spills) against 32.0 / 30.1: the
+// FP32 passes keep the load/store-unit kernel.
+// fields: element type, bytes, log2 digit base, mode, sign, log2 L, log2 W,
+// threads, CTAs per SM, pipelined, default
+#define PAC_COLTMA_LIST(X)                                 \
+  X(double, 8, 1, MODE_DIF, -1, 11, 2, 512, 1, 0, 0)       \
+  X(double, 8, 1, MODE_DIT, +1, 11, 2, 512, 1, 0, 0)       \
+  X(float, 4, 1, MODE_DIF, -1, 11, 3, 512, 1, 0, 0)        \
+  X(float, 4, 1, MODE_DIT, +1, 11, 3, 512, 1, 0, 0)        \
+  X(double, 8, 1, MODE_DIF, -1, 11, 1, 256, 2, 0, 0)       \
+  X(double, 8, 1, MODE_DIT, +1, 11, 1, 256, 2, 0, 0)       \
+  X(float, 4, 1, MODE_DIF, -1, 11, 2, 256, 2, 0, 0)        \
+  X(float, 4, 1, MODE_DIT, +1, 11, 2, 256, 2, 0, 0)        \
+  X(double, 8, 1, MODE_DIF, -1, 11, 2, 512, 1, 1, 1)       \
+  X(double, 8, 1, MODE_DIT, +1, 11, 2, 512, 1, 1, 1)       \
+  X(float, 4, 1, MODE_DIF, -1, 11, 3, 512, 1, 1, 0)        \
+  X(float, 4, 1, MODE_DIT, +1, 11, 3, 512, 1, 1, 0)
+
+// the variant-th candidate of a geometry (variant < 0: its default entry);
+// *cand returns its 1-based candidate number
+inline bool coltma_geometry(int bytes, int b2, int mode, int sign, int logL, int* logW, int* nt,
+                            int* minb, int* pipe, int variant, int* cand) {
+  int seen = 0;
+#define PAC_X(T, BY, B2_, MO, SG, LL, LW, NT_, MB, PP, DF)                                \
+  if (bytes == BY && b2 == B2_ && mode == MO && sign == SG && logL == LL &&            \
+      (variant < 0 ? (++seen, DF == 1) : seen++ == variant)) {                         \
+    *logW = LW;                                                                        \
+    *nt = NT_;                                                                         \
+    *minb = MB;                                                                        \
+    *pipe = PP;                                                                        \
+    *cand = variant < 0 ? seen : variant + 1;                                          \
+    return true;                                                                       \
+  }
+  PAC_COLTMA_LIST(PAC_X)
+#undef PAC_X
+  return false;
+}
+
 // Work-queue fast paths (pac_queue_kernel, 256 threads): multi-plan passes
 // of these geometries get their tile width and run the compile-time body
 // (pass_body_ct) inside the persistent queue kernel; all others run the

@@ -102,6 +102,37 @@ PAC_HD Cx<T> tw4_value(const PassDesc& d, long long cta, int w, int e) {
   return cmul(ld_tw(lo + (E & ((1u << d.tw4_lolog) - 1))), ld_tw(hi + (E >> d.tw4_lolog)));
 }
 
+// The stage twiddles w_K^{j s}, s = 1 .. R-1, of a butterfly with index j
+// (tw points at entry j of the stage table, which is s-major: entry
+// (s-1)*ell + j).  FP64 reads only the powers of two w^j, w^2j, w^4j, w^8j
+// and forms every other power as a product of two already formed ones
+// (w^s = w^hb * w^(s-hb), hb the highest power of two in s: at most three
+// roundings deep, ~1e-15 relative) -- a load per twiddle costs more issue
+// slots and load-queue space than the FP64 product, whose pipe the passes
+// leave mostly idle.  FP32 reads every entry: its table values are rounded
+// once from FP64 and are used as they are.
+template <typename T, int R>
+PAC_HD void stage_twiddles(const Cx<T>* tw, int ell, Cx<T> (&w)[R]) {
+  if constexpr (sizeof(T) == 8 && R >= 4) {
+    static_for<ilog2(R)>([&](auto b) {
+      constexpr int s = 1 << b.value;
+      w[s] = ld_tw(tw + (s - 1) * ell);
+    });
+    static_for<R>([&](auto ss) {
+      constexpr int s = ss.value;
+      if constexpr (s > 2 && (s & (s - 1)) != 0) {
+        constexpr int hb = 1 << ilog2(s);
+        w[s] = cmul(w[hb], w[s - hb]);
+      }
+    });
+  } else {
+    static_for<R - 1>([&](auto ss) {
+      constexpr int s = ss.value + 1;
+      w[s] = ld_tw(tw + (s - 1) * ell);
+    });
+  }
+}
+
 // The arithmetic of one radix-R butterfly on registers x: DIT pre-twiddles,
 // the R-point DFT, DIF post-twiddles.  x[m] holds the element at input slot
 // m (DIF: m, DIT: sigma_b(m)); afterwards register p holds output index
@@ -125,9 +156,11 @@ PAC_HD void bf_math(const PassDesc& d, long long cta, Cx<T> (&x)[R], int w, int 
       });
     }
     if (twiddle) {
+      Cx<T> wv[R];
+      stage_twiddles<T, R>(tw, ell, wv);
       static_for<R - 1>([&](auto ss) {
         constexpr int s = ss.value + 1;
-        x[s] = ctw(x[s], ld_tw(tw + (s - 1) * ell), SIGN);
+        x[s] = ctw(x[s], wv[s], SIGN);
       });
     }
   }
@@ -135,9 +168,11 @@ PAC_HD void bf_math(const PassDesc& d, long long cta, Cx<T> (&x)[R], int w, int 
   // register p now holds output index brev(p)
   if constexpr (DIF) {
     if (twiddle) {
+      Cx<T> wv[R];
+      stage_twiddles<T, R>(tw, ell, wv);
       static_for<R>([&](auto pp) {
         constexpr int s = brev_c(pp.value, LR);
-        if constexpr (s > 0) x[pp.value] = ctw(x[pp.value], ld_tw(tw + (s - 1) * ell), SIGN);
+        if constexpr (s > 0) x[pp.value] = ctw(x[pp.value], wv[s], SIGN);
       });
     }
     // 4-step post-twiddle: only the innermost stage of a DIF pass

@@ -190,6 +190,22 @@ PAC_API int pac_convolve(pac_plan_t plan, const void* x_re, const void* x_im,
                          const void* hhat_re, const void* hhat_im, int hhat_per_problem,
                          void* y_re, void* y_im, double scale, pac_stream_t stream);
 
+/* Bounded device waits.  Kernels that wait on an mbarrier for their tensor
+ * copies (the tensor-copy column passes, the opt-in pipelined column kernel)
+ * give up after a limit of SM clock cycles instead of spinning forever: a
+ * CTA whose wait gives up writes PAC_ERROR_TIMEOUT into the plan's device
+ * status word, issues nothing more, lets the copies it has in flight land
+ * and leaves -- the output of that call is then incomplete, and the device
+ * stays usable.  pac_plan_check_status synchronises `stream`, reads and
+ * clears the status word and returns PAC_ERROR_TIMEOUT if a wait of any
+ * call of this plan gave up since the last check (PAC_SUCCESS otherwise);
+ * the fft.h functions check it after every call.  pac_plan_set_wait_limit
+ * sets the limit, in SM cycles, for the plan's later calls (<= 0: the
+ * default 2^31, about a second); a tiny limit makes the waits run out.
+ * No counterpart in the reference (whose calls never wait on a device). */
+PAC_API int pac_plan_set_wait_limit(pac_plan_t plan, long long cycles);
+PAC_API int pac_plan_check_status(pac_plan_t plan, pac_stream_t stream);
+
 /* One operator over all axes of every problem, in -> out (may alias).
  * See PAC_OP_*.  For PAC_OP_FFT / PAC_OP_IFFT an axis split over several
  * passes needs the plan workspace (allocated on first use). */
@@ -232,7 +248,11 @@ PAC_API int pac_convolve_1d_noalloc(const double* x_re, const double* x_im, cons
  * launches are captured once into a CUDA graph per set of buffer addresses
  * and replayed afterwards (the first call for new addresses captures; later
  * calls launch the graph).  Calls on one multi-plan are serialised by a
- * lock. */
+ * lock on the host, but its work-queue counters are one device block per
+ * multi-plan: calls whose device work overlaps (different streams, or graph
+ * replays on different streams) take items from the same counters and
+ * corrupt each other's results.  Queue the calls of one multi-plan on one
+ * stream, or use one multi-plan per stream. */
 typedef struct pac_multi_s* pac_multi_t;
 
 /* ranks[p] in 1..3; dims holds 3 entries per problem (the first ranks[p]

@@ -56,9 +56,17 @@ def build_orc(force=False):
     return so
 
 
-def build_ref(ref_dir="/root/reference"):
+def ref_source_dir():
+    """The reference's source directory: the environment variable PAC_REF_DIR
+    (unset: none -- the checkers that need it are skipped)."""
+    d = os.environ.get("PAC_REF_DIR")
+    return d if d and os.path.isdir(d) else None
+
+
+def build_ref(ref_dir=None):
     """Compile the reference sources into _ref/ (only where they exist)."""
-    if not os.path.isdir(ref_dir):
+    ref_dir = ref_dir or ref_source_dir()
+    if not ref_dir or not os.path.isdir(ref_dir):
         return None
     subprocess.check_call(["make", "-s", "-C", HERE, "ref", f"REF_DIR={ref_dir}"])
     return os.path.join(HERE, "_ref", "libref.so")

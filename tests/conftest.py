@@ -39,8 +39,8 @@ def orc():
 def ref():
     path = os.path.join(ROOT, "oracle", "_ref", "libref.so")
     if not os.path.exists(path):
-        if os.path.isdir("/root/reference"):
-            O.build_ref("/root/reference")
+        if O.ref_source_dir():  # PAC_REF_DIR names the reference sources
+            O.build_ref()
         else:
             pytest.skip("reference library not built here")
     return O.Ref(path)

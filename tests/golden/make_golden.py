@@ -6,7 +6,7 @@ own sources by ``oracle/Makefile`` (target ``ref``), on seeded inputs.
 
 Run from the repository root where the reference sources are present:
 
-    python tests/golden/make_golden.py [/path/to/reference]
+    python tests/golden/make_golden.py REF_DIR   (or PAC_REF_DIR=... python ...)
 
 Each case (shape, radix) is one ``.npz`` holding the inputs and every
 output of the path: the three butterfly operators (A, conj(A), A^T), the
@@ -43,8 +43,9 @@ def case_name(shape, r):
     return "g_" + "x".join(str(s) for s in shape) + f"_r{r}.npz"
 
 
-def make(ref_dir="/root/reference"):
-    O.build_ref(ref_dir)
+def make(ref_dir):
+    if not O.build_ref(ref_dir):
+        raise SystemExit(f"no reference sources at {ref_dir!r}")
     ref = O.Ref()
     for idx, (shape, r) in enumerate(CASES):
         rng = np.random.default_rng(1000 + idx)
@@ -70,4 +71,8 @@ def make(ref_dir="/root/reference"):
 
 
 if __name__ == "__main__":
-    make(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    # the reference's source directory: the first argument, else PAC_REF_DIR
+    src = sys.argv[1] if len(sys.argv) > 1 else O.ref_source_dir()
+    if not src:
+        raise SystemExit("usage: make_golden.py REF_DIR (or set PAC_REF_DIR)")
+    make(src)

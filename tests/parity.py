@@ -183,18 +183,22 @@ def check_spectrum_orders(L, dims, batch, base, form):
                            rtol=tol, atol=tol * np.abs(pv).max())
 
 
-COLUMN_KERNELS = ("pipe", "tile", "cluster0", "cluster1")
+COLUMN_KERNELS = ("pipe", "tile", "cluster0", "cluster1", "tma1", "tma2", "tma3")
 
 
 def check_column_kernels(L, orc, dims, batch, form, monkeypatch, kind):
     """Column passes served by each column kernel give the oracle's results
     (the convolution, A^T, conj(A) and A): one-CTA tiles ("tile", the
-    default), the pipelined persistent kernel ("pipe", PAC_PIPE=1), or tiles
-    shared by a CTA cluster ("clusterK", PAC_CLUSTER_VARIANT=K)."""
+    default), the pipelined persistent kernel ("pipe", PAC_PIPE=1), tiles
+    shared by a CTA cluster ("clusterK", PAC_CLUSTER_VARIANT=K), or tiles
+    staged by tensor copies ("tmaK", the K-th candidate, PAC_COLTMA=K)."""
     monkeypatch.delenv("PAC_CLUSTER_VARIANT", raising=False)
     monkeypatch.delenv("PAC_PIPE", raising=False)
+    monkeypatch.setenv("PAC_COLTMA", "0")
     if kind == "pipe":
         monkeypatch.setenv("PAC_PIPE", "1")
+    elif kind.startswith("tma"):
+        monkeypatch.setenv("PAC_COLTMA", kind[len("tma"):])
     elif kind.startswith("cluster"):
         monkeypatch.setenv("PAC_CLUSTER_VARIANT", kind[len("cluster"):])
     g = rng(31)
@@ -209,6 +213,48 @@ def check_column_kernels(L, orc, dims, batch, form, monkeypatch, kind):
         for b in range(batch):
             zr, zi = orc.butterflies(oop, 2, x[b].real, x[b].imag)
             assert crel(t[b], zr + 1j * zi) < TOL
+
+
+def check_wait_timeout(L, form, monkeypatch, kind="tma1"):
+    """Bounded waits: with a wait limit of a few SM cycles every tensor-copy
+    wait of the column passes gives up; the call reports PAC_ERROR_TIMEOUT
+    through pac_plan_check_status (the device stays usable), and the same
+    plan with the default limit convolves correctly afterwards."""
+    monkeypatch.setenv("PAC_COLTMA", "0")
+    monkeypatch.delenv("PAC_PIPE", raising=False)
+    if kind == "pipe":
+        monkeypatch.setenv("PAC_PIPE", "1")
+    else:
+        monkeypatch.setenv("PAC_COLTMA", kind[len("tma"):])
+    dims, batch = (2048, 64), 1
+    dt = np.float64 if form == pac.PAC_FORM_F64 else np.float32
+    g = rng(41)
+    x = g.standard_normal((batch,) + dims) + 1j * g.standard_normal((batch,) + dims)
+    h = g.standard_normal(dims) + 1j * g.standard_normal(dims)
+    d = Dev(L)
+    try:
+        plan = pac.Plan(L, dims, batch, 2, form)
+        assert L.pac_plan_check_status(plan.h, None) == 0
+        hr, hi = d.put(h.real), d.put(h.imag)
+        Hr, Hi = d.zeros(dims, dt), d.zeros(dims, dt)
+        plan.filter_spectrum(hr, hi, Hr, Hi)
+        xr, xi = d.put(x.real.astype(dt)), d.put(x.imag.astype(dt))
+        yr, yi = d.zeros((batch,) + dims, dt), d.zeros((batch,) + dims, dt)
+        pac.check(L, L.pac_plan_set_wait_limit(plan.h, 4), "wait limit")
+        plan.convolve(xr, xi, Hr, Hi, yr, yi)
+        assert L.pac_plan_check_status(plan.h, None) == 8  # PAC_ERROR_TIMEOUT
+        assert b"gave up" in L.pac_last_error()
+        assert L.pac_plan_check_status(plan.h, None) == 0  # read and cleared
+        pac.check(L, L.pac_plan_set_wait_limit(plan.h, 0), "wait limit")
+        plan.convolve(xr, xi, Hr, Hi, yr, yi)
+        assert L.pac_plan_check_status(plan.h, None) == 0
+        y = d.get(yr, (batch,) + dims, dt) + 1j * d.get(yi, (batch,) + dims, dt)
+        plan.close()
+    finally:
+        d.free()
+    tol = TOL if form == pac.PAC_FORM_F64 else TOL_F32
+    assert crel(y, fftconv(x, h[None], (1, 2))) < tol
+    assert L.pac_plan_set_wait_limit(None, 1) == 1  # PAC_ERROR_INVALID_VALUE
 
 
 def check_multi(L, shapes, form, stream=False, seed=3, tune=None):

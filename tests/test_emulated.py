@@ -177,6 +177,15 @@ def test_column_kernels(emu, orc, monkeypatch, form, kind):
     P.check_column_kernels(emu, orc, (2048, 32), 2, form, monkeypatch, kind)
 
 
+@pytest.mark.parametrize("kind", ["tma1", "tma2", "tma3", "pipe"])
+@pytest.mark.parametrize("form", [0, 1])
+def test_wait_timeout_reported(emu, monkeypatch, form, kind):
+    """The replay models a tensor copy as landing 1000 cycles after it is
+    issued: a wait limit of 4 cycles gives up, and the status word, its
+    read-and-clear and the recovery run through the host plan layer."""
+    P.check_wait_timeout(emu, form, monkeypatch, kind)
+
+
 @pytest.mark.parametrize("form", [0, 1])
 def test_multi_uneven_batch(emu, form):
     """Many convolutions of uneven 1D/2D/3D shapes through the work-queue

@@ -234,6 +234,16 @@ def test_column_kernels(lib, orc, monkeypatch, form, kind):
 
 
 
+@pytest.mark.parametrize("kind", ["tma1", "tma2", "tma3", "pipe"])
+@pytest.mark.parametrize("form", [0, 1])
+def test_wait_timeout_reported(lib, monkeypatch, form, kind):
+    """A wait limit of 4 SM cycles: every bounded tensor-copy wait of the
+    column passes gives up before its copy lands; the kernels report
+    PAC_ERROR_TIMEOUT in the plan's status word, let the copies land and
+    leave; the device stays usable and the next call is correct."""
+    P.check_wait_timeout(lib, form, monkeypatch, kind)
+
+
 @pytest.mark.parametrize("form", [0, 1])
 @pytest.mark.parametrize("stream", [False, True])
 def test_multi_uneven_batch(lib, form, stream):
