@@ -26,6 +26,7 @@ int be_stream_destroy(void* s);
 int be_stream_sync(void* s);
 int be_stream_wait(void* waiter, void* waitee);
 int be_l2_persist(void* stream, const void* base, size_t bytes);
+long long be_l2_bytes();  // L2 cache size of the current device (0: none / unknown)
 // timing events: record on a stream, elapsed milliseconds between two
 int be_event_create(void** ev);
 int be_event_destroy(void* ev);

@@ -490,6 +490,14 @@ int be_stream_sync(void* s) {
   PAC_CU(cudaStreamSynchronize((cudaStream_t)s), "cudaStreamSynchronize");
   return PAC_SUCCESS;
 }
+long long be_l2_bytes() {
+  int dev = 0, n = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&n, cudaDevAttrL2CacheSize, dev) != cudaSuccess || n < 0)
+    return 0;
+  return n;
+}
+
 int be_l2_persist(void* stream, const void* base, size_t bytes) {
   int dev = 0;
   PAC_CU(cudaGetDevice(&dev), "cudaGetDevice");

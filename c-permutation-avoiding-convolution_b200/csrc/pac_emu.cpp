@@ -56,6 +56,7 @@ int be_stream_destroy(void*) { return PAC_SUCCESS; }
 int be_stream_sync(void*) { return PAC_SUCCESS; }
 int be_stream_wait(void*, void*) { return PAC_SUCCESS; }
 int be_l2_persist(void*, const void*, size_t) { return PAC_SUCCESS; }
+long long be_l2_bytes() { return 0; }
 // events: host clock readings (the replay runs synchronously, so two
 // readings bracket the work issued between them)
 int be_event_create(void** ev) {

@@ -19,6 +19,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "pac.h"
 #include "pac_backend.h"
 
@@ -207,14 +209,21 @@ static int issue_levels(pac_multi_s* m, void* stream, void** ev = nullptr) {
     const auto& groups = m->levels[k];
     unsigned long long* c = cnt + k * kGroups;
     if (ev) PAC_TRY(be_event_record(ev[k], stream));
+    // one NVTX range per level, named as bench.py's per-level breakdown
+    char name[48];
+    snprintf(name, sizeof(name), "pac multi level %d", (int)k);
+    nvtxRangePushA(name);
+    int st = PAC_SUCCESS;
     if (groups.size() == 1) {
-      PAC_TRY(launch_group(m, groups[0], c, stream));
-      continue;
+      st = launch_group(m, groups[0], c, stream);
+    } else {
+      st = be_stream_wait(m->side, stream);
+      if (st == PAC_SUCCESS) st = launch_group(m, groups[0], c, stream);
+      if (st == PAC_SUCCESS) st = launch_group(m, groups[1], c + 1, m->side);
+      if (st == PAC_SUCCESS) st = be_stream_wait(stream, m->side);
     }
-    PAC_TRY(be_stream_wait(m->side, stream));
-    PAC_TRY(launch_group(m, groups[0], c, stream));
-    PAC_TRY(launch_group(m, groups[1], c + 1, m->side));
-    PAC_TRY(be_stream_wait(stream, m->side));
+    nvtxRangePop();
+    PAC_TRY(st);
   }
   if (ev) PAC_TRY(be_event_record(ev[m->levels.size()], stream));
   return PAC_SUCCESS;

@@ -34,6 +34,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "pac.h"
 #include "pac_backend.h"
 #include "pac_special.h"
@@ -497,9 +499,24 @@ static size_t pass_smem(const PassSpec& p) {
   return (d.nst == 1 && !d.nat && !d.pipe && d.logC == 0) ? 0 : p.smem;
 }
 
-static int launch(const Schedule& s, PassSpec& p, void* stream) {
+// NVTX range name of a pass: its mode and line length, as bench.py names
+// the passes of its per-pass breakdown ("DIF factor k", "fused innermost",
+// "DIT factor k")
+static void pass_range_name(const PassDesc& d, int index, char* buf, size_t n) {
+  const char* mode = d.mode == MODE_CONV ? "fused innermost: DIF, x Hhat, DIT"
+                     : d.mode == MODE_DIF ? "DIF" : "DIT";
+  snprintf(buf, n, "pac pass %d %s 2^%d%s%s", index, mode, d.logL, d.logS > 0 ? " columns" : "",
+           d.tma ? " (tensor copies)" : "");
+}
+
+static int launch(const Schedule& s, PassSpec& p, void* stream, int index = 0) {
   p.smem = pass_smem(p);
-  return be_launch_pass(p.d, s.bytes, p.b2, p.grid, p.threads, p.smem, stream);
+  char name[96];
+  pass_range_name(p.d, index, name, sizeof(name));
+  nvtxRangePushA(name);
+  const int st = be_launch_pass(p.d, s.bytes, p.b2, p.grid, p.threads, p.smem, stream);
+  nvtxRangePop();
+  return st;
 }
 
 // Launch a pass list; with pass timing enabled, bracket every pass with
@@ -512,7 +529,7 @@ static int exec_passes(pac_plan_s* pl, const Schedule& s, std::vector<PassSpec>&
     apply_special(s, p);
   }
   if (!pl->timing) {
-    for (auto& p : passes) PAC_TRY(launch(s, p, stream));
+    for (size_t i = 0; i < passes.size(); ++i) PAC_TRY(launch(s, passes[i], stream, (int)i));
     return PAC_SUCCESS;
   }
   std::lock_guard<std::mutex> g(pl->t_mu);
@@ -528,7 +545,7 @@ static int exec_passes(pac_plan_s* pl, const Schedule& s, std::vector<PassSpec>&
   }
   PAC_TRY(be_event_record(pl->t_ev[0], stream));
   for (size_t i = 0; i < n; ++i) {
-    PAC_TRY(launch(s, passes[i], stream));
+    PAC_TRY(launch(s, passes[i], stream, (int)i));
     PAC_TRY(be_event_record(pl->t_ev[i + 1], stream));
   }
   for (size_t i = 0; i < n; ++i) {

@@ -142,6 +142,9 @@ PAC_API int pac_plan_create_tuned(pac_plan_t* plan, int rank, const int* dims,
  * returns the fastest.  With cache_path non-NULL it first looks the
  * problem up there and, when it tuned, appends the result as one JSON line
  * ({"key": ..., "max_factor_log": ..., ..., "ms": ..., "default_ms": ...}).
+ * While it times, the output buffer (the passes' intermediate) is kept
+ * persisting in L2 when it fits in three quarters of L2, so a knob set is
+ * timed under the cache policy of a caller that does the same.
  * No counterpart in the reference. */
 typedef struct {
   pac_tune_t tune;     /* the fastest knobs                               */
