@@ -511,7 +511,7 @@ def parse_knobs(text):
     """--knobs "max_radix_log=3,w_shift=1": explicit pac_tune_t knobs (the rest 0)."""
     if not text:
         return None
-    knobs = {"max_factor_log": 0, "max_radix_log": 0, "special": 0, "w_shift": 0}
+    knobs = {"max_factor_log": 0, "max_radix_log": 0, "special": 0, "w_shift": 0, "plane": 0}
     for item in text.split(","):
         k, v = item.split("=")
         if k.strip() not in knobs:

@@ -257,7 +257,7 @@ def dropin_twiddles(L, r, n):
 class Tune(C.Structure):
     """pac_tune_t: plan knobs (0 everywhere = the built-in choices)"""
     _fields_ = [("max_factor_log", C.c_int), ("max_radix_log", C.c_int), ("special", C.c_int),
-                ("w_shift", C.c_int)]
+                ("w_shift", C.c_int), ("plane", C.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

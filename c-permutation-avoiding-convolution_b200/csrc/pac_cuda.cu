@@ -39,6 +39,9 @@ void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 // the tensor-copy column passes (pac_coltma.cu)
 int launch_coltma(const PassDesc& d, int elem_bytes, int b2, long long grid, int threads,
                   size_t smem, void* stream);
+// the plane passes of 3D convolutions (pac_plane.cu)
+int launch_plane(const PassDesc& d, int elem_bytes, int b2, long long grid, int threads,
+                 size_t smem, void* stream);
 
 static int cuda_fail(cudaError_t e, const char* what) {
   return set_error(PAC_ERROR_CUDA, "%s: %s", what, cudaGetErrorString(e));
@@ -844,6 +847,7 @@ static int launch_pipe(const PassDesc& d, int elem_bytes, int b2, long long grid
 
 int be_launch_pass(const PassDesc& d, int elem_bytes, int b2, long long grid, int threads,
                    size_t smem, void* stream) {
+  if (d.plane) return launch_plane(d, elem_bytes, b2, grid, threads, smem, stream);
   if (d.tma) return launch_coltma(d, elem_bytes, b2, grid, threads, smem, stream);
   if (d.pipe) return launch_pipe(d, elem_bytes, b2, grid, threads, smem, stream);
   if (d.logC > 0) return launch_cluster(d, elem_bytes, b2, grid, threads, smem, stream);

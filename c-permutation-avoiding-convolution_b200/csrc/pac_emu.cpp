@@ -302,8 +302,51 @@ static int replay_coltma(const PassDesc& d, long long grid) {
   return PAC_SUCCESS;
 }
 
+// replay of a plane pass (pac_plane.cuh): each cluster's CTAs get their own
+// shared-memory image (NaN at the start, so that a read of a slot no stage
+// wrote shows up in the results); every phase runs for all ranks of the
+// cluster before the next one starts, as the cluster barriers order them.
+template <typename T, int B2, int L1, int L2, int LC, int NT>
+static int replay_plane(const PassDesc& d, long long grid) {
+  using G = PlaneGeo<T, B2, L1, L2, LC, NT>;
+  constexpr int C = G::C;
+  const size_t per = (size_t)2 * G::RC * G::P2;
+  std::vector<T> sm(per * C);
+  std::vector<long long> lb((size_t)G::RC * C);
+  ClView<T, C> cv;
+  for (int r = 0; r < C; ++r) {
+    cv.re[r] = sm.data() + per * r;
+    cv.im[r] = cv.re[r] + (size_t)G::RC * G::P2;
+  }
+  if (grid % C) return set_error(PAC_ERROR_INTERNAL, "plane pass grid %lld", grid);
+  for (long long plane = 0; plane < grid / C; ++plane) {
+    std::fill(sm.begin(), sm.end(), std::numeric_limits<T>::quiet_NaN());
+    for (int r = 0; r < C; ++r)
+      for (int i = 0; i < G::RC; ++i)
+        lb[(size_t)r * G::RC + i] = (plane << (L1 + L2)) + ((long long)(r * G::RC + i) << L2);
+    for (int phase = 0; phase < 3; ++phase)
+      for (int r = 0; r < C; ++r) {
+        cv.rank = r;
+        plane_body<T, B2, L1, L2, LC, NT>(d, plane, cv.re[r], cv.im[r], cv,
+                                          lb.data() + (size_t)r * G::RC, phase);
+      }
+  }
+  return PAC_SUCCESS;
+}
+
 int be_launch_pass(const PassDesc& d, int elem_bytes, int b2, long long grid, int threads,
                    size_t, void*) {
+  if (d.plane) {
+#define PAC_X(T, BY, B2_, L1_, L2_, LC, NT_, MB)                                           \
+  if (elem_bytes == BY && b2 == B2_ && d.plane_logN1 == L1_ && d.plane_logN2 == L2_ &&   \
+      threads == NT_) {                                                                  \
+    g_launches++;                                                                        \
+    return replay_plane<T, B2_, L1_, L2_, LC, NT_>(d, grid);                             \
+  }
+    PAC_PLANE_LIST(PAC_X)
+#undef PAC_X
+    return set_error(PAC_ERROR_INTERNAL, "no plane replay for a pass marked plane");
+  }
   if (d.tma) {
     int seen = 0;  // candidates of this geometry so far; d.tma - 1 picks one
 #define PAC_X(T, BY, B2_, MO, SG, LL, LW, NT_, MB, PP, DF)                                      \

@@ -100,6 +100,13 @@ struct PassDesc {
   // k > 0: column pass staged through shared memory by tensor copies, the
   // k-th geometry of its kind on PAC_COLTMA_LIST (pac_special.h; ColTma)
   int tma;
+  // 1: plane pass of a 3D convolution (pac_plane.cuh): axes 1 and 2 of
+  // every plane, whose stages are rlog[0 .. plane_n1s-1] (axis 1) then
+  // rlog[plane_n1s .. nst-1] (axis 2), on a cluster of 2^logC CTAs
+  int plane;
+  int plane_n1s;
+  int plane_logN1;
+  int plane_logN2;
   // 1: tensor-core form, radix-16 stages on the tensor cores (pac_tc.cuh);
   // tcc: their DFT operands, per stage kind and lane (tc_const_set)
   int tc;
@@ -348,3 +355,4 @@ PAC_HD void nat_line(const PassDesc& d, long long g, long long* in_base, long lo
 }  // namespace pac
 #include "pac_stages.cuh"
 #include "pac_coltma.cuh"
+#include "pac_plane.cuh"

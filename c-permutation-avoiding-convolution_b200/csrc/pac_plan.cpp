@@ -82,6 +82,7 @@ struct Schedule {
   int rlog_cap = 4;
   int special = 0;
   int w_shift = 0;
+  int plane = 0;        // 3D: 1 plane schedule, -1 line schedule, 0 built-in
   void* tcc = nullptr;  // its DFT operand table (tensor-core form)
   std::vector<VAx> vax;
   std::vector<std::vector<int>> rad;  // per factor: stage radix logs, DIF order
@@ -256,7 +257,7 @@ struct pac_plan_s {
   int b2s[3] = {1, 1, 1};    // every axis's
   int form = PAC_FORM_F64;
   long long N = 1;
-  pac_tune_t tune = {0, 0, 0, 0};         // knobs the plan was built with
+  pac_tune_t tune = {0, 0, 0, 0, 0};      // knobs the plan was built with
   pac::Schedule main;                     // storage type of the form
   std::unique_ptr<pac::Schedule> s64;     // FP64 schedule (F32 form: filter spectrum)
   std::mutex ws_mu;
@@ -375,7 +376,7 @@ static PassSpec make_pass(const Schedule& s, int vi, long long batch, long long 
 static void apply_special(const Schedule& s, PassSpec& p) {
   PassDesc& d = p.d;
   int logW = 0, nt = 0;
-  if (d.nat) return;
+  if (d.nat || d.plane) return;
   if (s.special < 0) return;  // tuned off
   // column pass whose tile a CTA cluster shares (W columns within the
   // stride, whole tiles), opt-in: PAC_CLUSTER_VARIANT=k picks the k-th
@@ -654,13 +655,106 @@ static int run_transform(pac_plan_s* pl, const Schedule& s, int op, long long ba
 
 // The passes of one convolution call (2m - 1 for m factors): DIF over the
 // outer factors, the fused innermost pass, DIT back; all in place in y.
+// The plane schedule of a 3D convolution (pac_plane.cuh): the knob plane
+// (or, at its built-in 0, PAC_PLANE=1/0; unset: on for FP32 storage, off for
+// FP64), one factor per axis, the default radix schedules, and a plane
+// kernel compiled for the (N1, N2) planes.  Measured on FP32 256^3: 35% fewer
+// DRAM bytes per convolution and the same time as the line schedule; on
+// 512 x 256 x 128: 13% faster.
+static bool plane_active(const Schedule& s, int* logC = nullptr, int* nt = nullptr) {
+  int want = s.plane;
+  if (want == 0) {
+    const char* e = getenv("PAC_PLANE");
+    want = e ? (atoi(e) ? 1 : -1) : (s.bytes == 4 ? 1 : -1);
+  }
+  if (want <= 0 || s.tc || s.rlog_cap < 4 || s.vax.size() != 3) return false;
+  for (int i = 0; i < 3; ++i)
+    if (!s.vax[i].first || !s.vax[i].last || s.vax[i].axis != i) return false;
+  const int b2 = s.vax[1].b2;
+  if (s.vax[2].b2 != b2) return false;
+  int lc = 0, n = 0;
+  if (!plane_geometry(s.bytes, b2, s.vax[1].log, s.vax[2].log, &lc, &n)) return false;
+  if (s.rad[1] != radix_schedule(s.vax[1].log, b2) || s.rad[2] != radix_schedule(s.vax[2].log, b2))
+    return false;
+  if (logC) *logC = lc;
+  if (nt) *nt = n;
+  return true;
+}
+
+// The plane pass of a 3D plan over `batch` problems, in place in y: axes 1
+// and 2 of every plane, stages of axis 1 then axis 2 in rlog / tw_off.
+static PassSpec make_plane_pass(const Schedule& s, long long batch, long long N) {
+  int logC = 0, nt = 0;
+  plane_active(s, &logC, &nt);
+  PassSpec p = make_pass(s, 2, batch, N);
+  PassDesc& d = p.d;
+  const int log1 = s.vax[1].log, log2 = s.vax[2].log;
+  d.plane = 1;
+  d.plane_logN1 = log1;
+  d.plane_logN2 = log2;
+  d.plane_n1s = (int)s.rad[1].size();
+  d.nst = (int)(s.rad[1].size() + s.rad[2].size());
+  int k = 0;
+  for (int a = 1; a <= 2; ++a) {
+    int logK = s.vax[a].log;
+    for (int rl : s.rad[a]) {
+      d.rlog[k] = rl;
+      auto it = s.tw_off.find(std::make_pair(logK, rl));
+      d.tw_off[k] = it == s.tw_off.end() ? 0 : it->second;
+      logK -= rl;
+      ++k;
+    }
+  }
+  const int rc = 1 << (log1 - logC);
+  d.W = rc;
+  d.logW = log1 - logC;
+  d.pitch = pitch_for(s.bytes, log2, rc);
+  d.nthreads = nt;
+  p.threads = nt;
+  p.grid = ((batch * N) >> (log1 + log2)) << logC;
+  p.smem = (size_t)2 * rc * d.pitch * s.bytes;
+  return p;
+}
+
 static void build_conv_passes(pac_plan_s* pl, const void* x_re, const void* x_im,
                               const void* h_re, const void* h_im, int per_problem, void* y_re,
-                              void* y_im, double scale, std::vector<PassSpec>& passes) {
+                              void* y_im, double scale, std::vector<PassSpec>& passes,
+                              bool allow_plane = true) {
   const Schedule& s = pl->main;
   const long long N = pl->N;
   const int m = (int)s.vax.size();
   const long long hmask = per_problem ? -1LL : (N - 1);
+  if (allow_plane && plane_active(s)) {
+    // DIF axis 0, the plane pass, DIT axis 0
+    PassSpec a = make_pass(s, 0, pl->batch, N);
+    a.d.mode = MODE_DIF;
+    a.d.sign = -1;
+    a.d.in_re = x_re;
+    a.d.in_im = x_im;
+    a.d.out_re = y_re;
+    a.d.out_im = y_im;
+    passes.push_back(a);
+    PassSpec p = make_plane_pass(s, pl->batch, N);
+    p.d.mode = MODE_CONV;
+    p.d.h_re = h_re;
+    p.d.h_im = h_im;
+    p.d.h_mask = hmask;
+    p.d.scale = scale;
+    p.d.in_re = y_re;
+    p.d.in_im = y_im;
+    p.d.out_re = y_re;
+    p.d.out_im = y_im;
+    passes.push_back(p);
+    PassSpec c = make_pass(s, 0, pl->batch, N);
+    c.d.mode = MODE_DIT;
+    c.d.sign = +1;
+    c.d.in_re = y_re;
+    c.d.in_im = y_im;
+    c.d.out_re = y_re;
+    c.d.out_im = y_im;
+    passes.push_back(c);
+    return;
+  }
   for (int vi = 0; vi < m - 1; ++vi) {
     PassSpec p = make_pass(s, vi, pl->batch, N);
     p.d.mode = MODE_DIF;
@@ -719,8 +813,8 @@ int plan_conv_descs(pac_plan_s* pl, const void* x_re, const void* x_im, const vo
                     const void* h_im, void* y_re, void* y_im, std::vector<PassDesc>& descs,
                     std::vector<long long>& ctas, std::vector<size_t>& smem) {
   std::vector<PassSpec> passes;
-  if (!pl->main.vax.empty())
-    build_conv_passes(pl, x_re, x_im, h_re, h_im, 0, y_re, y_im, 1.0, passes);
+  if (!pl->main.vax.empty())  // (the work queue runs line passes only)
+    build_conv_passes(pl, x_re, x_im, h_re, h_im, 0, y_re, y_im, 1.0, passes, false);
   for (auto& p : passes) apply_queue_special(pl->main, p);
   for (auto& p : passes) {
     p.smem = pass_smem(p);
@@ -734,7 +828,7 @@ int plan_bytes(pac_plan_s* pl) { return pl->main.bytes; }
 // the factor lengths and stage radices of the plan (the autotuner skips a
 // knob set whose schedule it has already timed)
 std::string plan_signature(pac_plan_s* pl) {
-  std::string sig;
+  std::string sig = plane_active(pl->main) ? "plane|" : "";
   for (size_t i = 0; i < pl->main.vax.size(); ++i) {
     sig += std::to_string(pl->main.vax[i].log) + ":";
     for (int r : pl->main.rad[i]) sig += std::to_string(r) + ",";
@@ -834,9 +928,10 @@ static int create_plan(pac_plan_t* plan, int rank, const int* dims, const int* d
                        int batch, int form, const pac_tune_t* tune) {
   if (!plan || !dims || !digit_bases || rank < 1 || rank > 3 || batch < 1)
     return set_error(PAC_ERROR_INVALID_VALUE, "pac_plan_create: invalid rank/dims/batch");
-  const pac_tune_t knobs = tune ? *tune : pac_tune_t{0, 0, 0, 0};
+  const pac_tune_t knobs = tune ? *tune : pac_tune_t{0, 0, 0, 0, 0};
   if (knobs.max_factor_log < 0 || knobs.max_factor_log > 13 || knobs.max_radix_log < 0 ||
-      knobs.max_radix_log > 4 || knobs.special < -1 || knobs.w_shift < -6 || knobs.w_shift > 6)
+      knobs.max_radix_log > 4 || knobs.special < -1 || knobs.w_shift < -6 || knobs.w_shift > 6 ||
+      knobs.plane < -1 || knobs.plane > 1)
     return set_error(PAC_ERROR_INVALID_VALUE,
                      "pac_plan_create: knobs out of range (factor log %d, radix log %d, "
                      "special %d, w shift %d)",
@@ -877,6 +972,7 @@ static int create_plan(pac_plan_t* plan, int rank, const int* dims, const int* d
   p->main.rlog_cap = knobs.max_radix_log > 0 ? knobs.max_radix_log : 4;
   p->main.special = knobs.special;
   p->main.w_shift = knobs.w_shift;
+  p->main.plane = knobs.plane;
   int bytes = form == PAC_FORM_F64 ? 8 : 4;
   st = build_schedule(p->main, rank, p->logs, b2s, bytes);
   if (st != PAC_SUCCESS) return st;
@@ -937,7 +1033,7 @@ PAC_API int pac_plan_get_info(pac_plan_t plan, pac_plan_info_t* info) {
   info->form = plan->form;
   info->element_bytes = plan->main.bytes;
   int m = (int)plan->main.vax.size();
-  info->conv_passes = m == 0 ? 1 : 2 * m - 1;
+  info->conv_passes = m == 0 ? 1 : plane_active(plan->main) ? 3 : 2 * m - 1;
   info->transform_passes = m == 0 ? 1 : m;
   info->workspace_bytes = plan->ws_bytes + plan->tmp64_bytes;
   info->tune = plan->tune;

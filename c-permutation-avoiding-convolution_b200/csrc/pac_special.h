@@ -148,7 +148,11 @@ namespace pac {
   X(double, 8, 1, MODE_DIF, -1, 11, 2, 512, 1, 1, 1)       \
   X(double, 8, 1, MODE_DIT, +1, 11, 2, 512, 1, 1, 1)       \
   X(float, 4, 1, MODE_DIF, -1, 11, 3, 512, 1, 1, 0)        \
-  X(float, 4, 1, MODE_DIT, +1, 11, 3, 512, 1, 1, 0)
+  X(float, 4, 1, MODE_DIT, +1, 11, 3, 512, 1, 1, 0)        \
+  X(float, 4, 1, MODE_DIF, -1, 11, 3, 1024, 1, 1, 0)       \
+  X(float, 4, 1, MODE_DIT, +1, 11, 3, 1024, 1, 1, 0)       \
+  X(float, 4, 1, MODE_DIF, -1, 11, 3, 1024, 1, 0, 0)       \
+  X(float, 4, 1, MODE_DIT, +1, 11, 3, 1024, 1, 0, 0)
 
 // the variant-th candidate of a geometry (variant < 0: its default entry);
 // *cand returns its 1-based candidate number
@@ -166,6 +170,28 @@ inline bool coltma_geometry(int bytes, int b2, int mode, int sign, int logL, int
     return true;                                                                       \
   }
   PAC_COLTMA_LIST(PAC_X)
+#undef PAC_X
+  return false;
+}
+
+// Plane passes of 3D convolutions (PassDesc.plane, pac_plane.cuh): axes 1
+// and 2 of every N1 x N2 plane in one launch on a cluster of 2^LOGC CTAs.
+// fields: element type, bytes, log2 digit base, log2 N1, log2 N2, log2
+// cluster size, threads, CTAs per SM
+#define PAC_PLANE_LIST(X)                          \
+  X(float, 4, 1, 8, 8, 3, 256, 2)                  \
+  X(float, 4, 1, 8, 7, 2, 256, 2)                  \
+  X(double, 8, 1, 8, 8, 3, 256, 1)                 \
+  X(double, 8, 1, 8, 7, 2, 256, 1)
+
+inline bool plane_geometry(int bytes, int b2, int logN1, int logN2, int* logC, int* nt) {
+#define PAC_X(T, BY, B2_, L1, L2, LC, NT_, MB)                                        \
+  if (bytes == BY && b2 == B2_ && logN1 == L1 && logN2 == L2) {                     \
+    *logC = LC;                                                                     \
+    *nt = NT_;                                                                      \
+    return true;                                                                    \
+  }
+  PAC_PLANE_LIST(PAC_X)
 #undef PAC_X
   return false;
 }

@@ -30,8 +30,12 @@ PAC_HD int sidx_col32(int e) { return e + (e >> 3) + 8 * (e >> 7); }
 
 // geometry policy; -1 = read from the PassDesc at run time.  TCL_ = 1: a
 // tile of the tensor-core form, whose column tiles keep the one-per-32 pad
-// (pitch_for gives them an odd pitch instead of sidx_col32)
-template <int LOGL_ = -1, int LOGW_ = -1, int PITCH_ = -1, int COLS_ = -1, int TCL_ = 0>
+// (pitch_for gives them an odd pitch instead of sidx_col32).  TR_ = 1: the
+// lines are the columns of a row-major shared-memory tile (element e of
+// line w at e * PITCH + sidx(w)), and consecutive threads always take
+// consecutive lines (the plane passes' local axis-1 stages)
+template <int LOGL_ = -1, int LOGW_ = -1, int PITCH_ = -1, int COLS_ = -1, int TCL_ = 0,
+          int TR_ = 0>
 struct Shape {
   static constexpr int kLogL = LOGL_;
   static constexpr int kLogW = LOGW_;
@@ -58,12 +62,15 @@ struct Shape {
   // threads take consecutive lines first: only where a stage touches global
   // memory of a column tile (coalesced rows of W elements)
   static PAC_HD bool wfast(const PassDesc& d, bool global_facing) {
-    return global_facing && cols(d);
+    if constexpr (TR_) return true;
+    else return global_facing && cols(d);
   }
   // shared-memory index of element e of line w: padded lines
   template <typename T>
   static PAC_HD int sm(const PassDesc& d, int w, int e) {
-    if constexpr (!TCL_ && col_pad32((int)sizeof(T), COLS_, LOGW_ >= 0 ? 1 << LOGW_ : 0))
+    if constexpr (TR_)
+      return e * pitch(d) + sidx<T>(w);
+    else if constexpr (!TCL_ && col_pad32((int)sizeof(T), COLS_, LOGW_ >= 0 ? 1 << LOGW_ : 0))
       return w * pitch(d) + sidx_col32(e);
     else
       return w * pitch(d) + sidx<T>(e);

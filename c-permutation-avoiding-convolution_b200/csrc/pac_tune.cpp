@@ -110,15 +110,16 @@ static bool cache_lookup(const char* path, const std::string& key, pac_tune_resu
   std::vector<char> line(4096);
   while (fgets(line.data(), (int)line.size(), f)) {
     if (strncmp(line.data(), want.c_str(), want.size()) != 0) continue;
-    long long a, b, c, d;
+    long long a, b, c, d, e = 0;
     double ms = 0, dms = 0;
     if (!json_int(line.data(), "max_factor_log", &a) || !json_int(line.data(), "max_radix_log", &b) ||
         !json_int(line.data(), "special", &c) || !json_int(line.data(), "w_shift", &d))
       continue;
+    json_int(line.data(), "plane", &e);  // absent in lines of older caches: 0
     json_num(line.data(), "ms", &ms);
     json_num(line.data(), "default_ms", &dms);
     memset(r, 0, sizeof(*r));
-    r->tune = pac_tune_t{(int)a, (int)b, (int)c, (int)d};
+    r->tune = pac_tune_t{(int)a, (int)b, (int)c, (int)d, (int)e};
     r->ms = ms;
     r->default_ms = dms;
     r->cached = 1;
@@ -134,9 +135,10 @@ static int cache_append(const char* path, const std::string& key, const pac_tune
   if (!f) return set_error(PAC_ERROR_INVALID_VALUE, "pac_autotune: cannot write %s", path);
   fprintf(f,
           "{\"key\": \"%s\", \"max_factor_log\": %d, \"max_radix_log\": %d, \"special\": %d, "
-          "\"w_shift\": %d, \"ms\": %.6g, \"default_ms\": %.6g, \"candidates\": %d}\n",
+          "\"w_shift\": %d, \"plane\": %d, \"ms\": %.6g, \"default_ms\": %.6g, "
+          "\"candidates\": %d}\n",
           key.c_str(), r.tune.max_factor_log, r.tune.max_radix_log, r.tune.special,
-          r.tune.w_shift, r.ms, r.default_ms, r.candidates);
+          r.tune.w_shift, r.tune.plane, r.ms, r.default_ms, r.candidates);
   fclose(f);
   return PAC_SUCCESS;
 }
@@ -230,7 +232,7 @@ static int time_calls(F run, void* stream, double* ms) {
 // the candidate.
 template <class M>
 static void descend(M measure, bool search_special, int bytes, pac_tune_result_t* r) {
-  pac_tune_t cur = {0, 0, 0, 0};
+  pac_tune_t cur = {0, 0, 0, 0, 0};
   double cur_ms = 0;
   std::vector<std::string> seen;
   r->candidates = 0;
@@ -260,6 +262,15 @@ static void descend(M measure, bool search_special, int bytes, pac_tune_result_t
     pac_tune_t t = cur;
     t.max_radix_log = 3;
     consider(t, false);
+  }
+  {
+    // 3D: the other of the plane and line schedules (a knob set that builds
+    // the same schedule as the current one is not timed twice)
+    pac_tune_t t = cur;
+    t.plane = 1;
+    consider(t, true);
+    t.plane = -1;
+    consider(t, true);
   }
   {
     const int lmax = bytes == 8 ? 12 : 13;

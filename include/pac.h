@@ -87,12 +87,17 @@ enum {
  *                   kernel of the pass's geometry where one exists; k > 0:
  *                   its k-th candidate
  *   w_shift         lines per CTA of generic passes times 2^w_shift
+ *   plane           3D convolutions: 1 runs axes 1 and 2 of every plane in
+ *                   one pass on a thread-block cluster (3 passes over HBM in
+ *                   all) where a plane kernel exists for the shape, -1 the
+ *                   line schedule (5 passes), 0 the built-in choice
  * No counterpart in the reference, which has one fixed schedule per radix. */
 typedef struct {
   int max_factor_log;
   int max_radix_log;
   int special;
   int w_shift;
+  int plane;
 } pac_tune_t;
 
 typedef struct {

@@ -183,7 +183,7 @@ def check_spectrum_orders(L, dims, batch, base, form):
                            rtol=tol, atol=tol * np.abs(pv).max())
 
 
-COLUMN_KERNELS = ("pipe", "tile", "cluster0", "cluster1", "tma1", "tma2", "tma3")
+COLUMN_KERNELS = ("pipe", "tile", "cluster0", "cluster1", "tma1", "tma2", "tma3", "tma4", "tma5")
 
 
 def check_column_kernels(L, orc, dims, batch, form, monkeypatch, kind):
@@ -255,6 +255,34 @@ def check_wait_timeout(L, form, monkeypatch, kind="tma1"):
     tol = TOL if form == pac.PAC_FORM_F64 else TOL_F32
     assert crel(y, fftconv(x, h[None], (1, 2))) < tol
     assert L.pac_plan_set_wait_limit(None, 1) == 1  # PAC_ERROR_INVALID_VALUE
+
+
+def check_plane(L, dims, batch, form, monkeypatch, per_problem=False, seed=8):
+    """The plane schedule of a 3D convolution (axes 1 and 2 of every plane in
+    one cluster pass: 3 passes) against numpy's FP64 FFT, through the
+    environment switch and through the plan knob; the knob plane = -1 keeps
+    the line schedule (5 passes)."""
+    monkeypatch.setenv("PAC_PLANE", "1")
+    g = rng(seed)
+    shape = (batch,) + tuple(dims)
+    x = g.standard_normal(shape) + 1j * g.standard_normal(shape)
+    hs = shape if per_problem else dims
+    h = g.standard_normal(hs) + 1j * g.standard_normal(hs)
+    z = fftconv(x, h if per_problem else h[None], (1, 2, 3))
+    tol = TOL if form == pac.PAC_FORM_F64 else TOL_F32
+    y = native_conv(L, dims, batch, 2, form, x, h, per_problem=per_problem)
+    assert crel(y, z) < tol
+    plan = pac.Plan(L, dims, batch, 2, form)
+    assert plan.info().conv_passes == 3
+    plan.close()
+    monkeypatch.delenv("PAC_PLANE")
+    knob = {"max_factor_log": 0, "max_radix_log": 0, "special": 0, "w_shift": 0, "plane": 1}
+    y = native_conv(L, dims, batch, 2, form, x, h, per_problem=per_problem, tune=knob)
+    assert crel(y, z) < tol
+    plan = pac.Plan(L, dims, batch, 2, form, tune=dict(knob, plane=-1))
+    assert plan.info().conv_passes == 5
+    plan.close()
+    return y
 
 
 def check_multi(L, shapes, form, stream=False, seed=3, tune=None):
@@ -418,7 +446,7 @@ def check_tuned(L, dims, batch, base, form, tune, seed=6):
     plan = pac.Plan(L, dims, batch, base, form, tune=tune)
     got = plan.info().tune.as_dict()
     plan.close()
-    assert got == tune
+    assert got == dict({"plane": 0}, **tune)  # knobs a dict leaves out are 0
     return crel(y, z)
 
 

@@ -177,6 +177,15 @@ def test_column_kernels(emu, orc, monkeypatch, form, kind):
     P.check_column_kernels(emu, orc, (2048, 32), 2, form, monkeypatch, kind)
 
 
+@pytest.mark.parametrize("dims,batch,form,per", [((2, 256, 256), 1, 1, False),
+                                                  ((2, 256, 128), 2, 1, True),
+                                                  ((2, 256, 256), 1, 0, False),
+                                                  ((2, 256, 128), 1, 0, False)])
+def test_plane_schedule(emu, monkeypatch, dims, batch, form, per):
+    """3D plane schedule, replayed cluster by cluster, against numpy."""
+    P.check_plane(emu, dims, batch, form, monkeypatch, per_problem=per)
+
+
 @pytest.mark.parametrize("kind", ["tma1", "tma2", "tma3", "pipe"])
 @pytest.mark.parametrize("form", [0, 1])
 def test_wait_timeout_reported(emu, monkeypatch, form, kind):

@@ -234,6 +234,18 @@ def test_column_kernels(lib, orc, monkeypatch, form, kind):
 
 
 
+@pytest.mark.parametrize("dims,batch,form,per", [((256, 256, 256), 1, 1, False),
+                                                  ((512, 256, 128), 1, 1, False),
+                                                  ((8, 256, 256), 3, 1, True),
+                                                  ((16, 256, 256), 1, 0, False),
+                                                  ((16, 256, 128), 2, 0, False)])
+def test_plane_schedule(lib, monkeypatch, dims, batch, form, per):
+    """3D plane schedule (cluster kernel, distributed shared memory for the
+    outermost axis-1 stage) at the C4 sizes and smaller FP64 shapes, against
+    numpy's FP64 FFT."""
+    P.check_plane(lib, dims, batch, form, monkeypatch, per_problem=per)
+
+
 @pytest.mark.parametrize("kind", ["tma1", "tma2", "tma3", "pipe"])
 @pytest.mark.parametrize("form", [0, 1])
 def test_wait_timeout_reported(lib, monkeypatch, form, kind):
