@@ -39,19 +39,35 @@ void count_launch();
 // loads the next tile.  The wait for a load is bounded: on a timeout the
 // CTA reports PAC_ERROR_TIMEOUT in the plan's status word, waits (bounded)
 // for the copy in flight to land and leaves.
-template <typename T, int B2, int MODE, int SIGN, int LOGL, int LOGW, int NT, int MINB>
+//
+// TC = 1 (the tensor-core form): the radix-16 steps run on the 5th-generation
+// tensor cores (ColTma::tc_prep / tc_finish): every warpgroup writes its 128
+// butterflies' A rows after the tile, one of its threads issues the MMAs
+// into the warpgroup's 32 tensor-memory columns and commits them to the
+// warpgroup's mbarrier, and each thread reads its butterfly's row back.
+// Warp 0 allocates the tensor memory at the start and frees it at the end.
+template <typename T, int B2, int MODE, int SIGN, int LOGL, int LOGW, int NT, int MINB,
+          int TC = 0>
 __global__ void __launch_bounds__(NT, MINB)
     pac_coltma_kernel(const PassDesc d, const __grid_constant__ CUtensorMap tin_re,
                       const __grid_constant__ CUtensorMap tin_im,
                       const __grid_constant__ CUtensorMap tout_re,
                       const __grid_constant__ CUtensorMap tout_im) {
-  using CT = ColTma<T, B2, MODE, SIGN, LOGL, LOGW, NT>;
+  using CT = ColTma<T, B2, MODE, SIGN, LOGL, LOGW, NT, TC>;
   constexpr int W = CT::W, TILE = CT::TILE, NS = CT::NS;
   constexpr bool DIF = CT::DIF;
   extern __shared__ unsigned char pac_smem_raw[];
   __shared__ __align__(8) uint64_t bar;
+  __shared__ __align__(8) uint64_t tbar[TC ? CT::NWG : 1];
+  __shared__ uint32_t tmem_slot;
   T* Bre = reinterpret_cast<T*>(((uintptr_t)pac_smem_raw + 1023) & ~(uintptr_t)1023);
   T* Bim = Bre + TILE;
+  // tensor-core form: per warpgroup the hi and lo A tiles, then the DFT
+  // operand's hi and lo tiles (32-bit words of two halves)
+  uint32_t* Aop = reinterpret_cast<uint32_t*>(Bim + TILE);
+  uint32_t* Vh = Aop + (TC ? CT::NWG * CT::UTILE : 0);
+  uint32_t* Vl = Vh + 512;
+  uint32_t tbase = 0, tph = 0;
   const int t = threadIdx.x;
   const long long ntiles = d.nlines >> LOGW;
   auto issue_load = [&](long long tl) {
@@ -88,9 +104,22 @@ __global__ void __launch_bounds__(NT, MINB)
   };
   if (t == 0) {
     mbar_init(&bar, 1);
+    if constexpr (TC) {
+      for (int g = 0; g < CT::NWG; ++g) mbar_init(&tbar[g], 1);
+    }
     fence_barrier_init();
   }
+  if constexpr (TC) {
+    for (int i = t; i < 512; i += NT) CT::tc_fill_v(i, Vh, Vl);
+    fence_proxy_async();  // the operand is read by the tensor cores
+    if (t < 32) tmem_alloc(&tmem_slot, 32 * CT::NWG);
+    tc5_fence_before();
+  }
   __syncthreads();
+  if constexpr (TC) {
+    tc5_fence_after();
+    tbase = tmem_slot;
+  }
   long long tile = blockIdx.x;
   if (t == 0 && tile < ntiles) issue_load(tile);
   uint32_t phase = 0;
@@ -108,7 +137,43 @@ __global__ void __launch_bounds__(NT, MINB)
     static_for<NS>([&](auto ss) {
       constexpr int S = ss.value;
       CT::template read<S>(t, Bre, Bim, x);
-      CT::template compute<S>(d, tile, t, x);
+      if constexpr (CT::tc_step(S)) {
+        const int g = t >> 7;
+        uint32_t* Ah = Aop + g * CT::UTILE;
+        uint32_t* Al = Ah + CT::UTILE / 2;
+        static_for<CT::TPW>([&](auto kk) {
+          int E = 0;
+          CT::template tc_prep<S>(d, t, kk.value, x, Ah, Al, E);
+          fence_proxy_async();  // the A rows are read by the tensor cores
+          warpgroup_sync(g);
+          if ((t & 127) == 0) {
+            tc5_fence_after();
+            const uint32_t idesc = umma_idesc_f16(CT::UM, CT::UN);
+            // Xlo.Vhi + Xhi.Vlo + Xhi.Vhi (small products first), K = 32 in
+            // two steps of 16
+#pragma unroll
+            for (int pr = 0; pr < 3; ++pr) {
+              const uint32_t* A = pr == 0 ? Al : Ah;
+              const uint32_t* B = pr == 1 ? Vl : Vh;
+#pragma unroll
+              for (int ks = 0; ks < 2; ++ks)
+                umma_f16(tbase + 32 * g, umma_desc((const char*)A + 256 * ks, 128, 512),
+                         umma_desc((const char*)B + 256 * ks, 128, 512), idesc,
+                         (pr | ks) != 0);
+            }
+            umma_commit(&tbar[g]);
+          }
+          if (!mbar_wait_bounded(&tbar[g], tph)) report_timeout(d);
+          tph ^= 1;
+          tc5_fence_after();
+          float D[32];
+          tmem_ld32(tbase + ((uint32_t)(32 * ((t >> 5) & 3)) << 16) + 32 * g, D);
+          CT::template tc_finish<S>(d, t, kk.value, D, E, x);
+          tc5_fence_before();
+        });
+      } else {
+        CT::template compute<S>(d, tile, t, x);
+      }
       if constexpr (CT::split_step(S)) __syncthreads();
       CT::template write<S>(d, t, Bre, Bim, x);
       if constexpr (S == NS - 1) fence_proxy_async();  // visible to the tensor store
@@ -121,6 +186,14 @@ __global__ void __launch_bounds__(NT, MINB)
     }
   }
   if (t == 0) bulk_wait_all();
+  if constexpr (TC) {
+    tc5_fence_before();
+    __syncthreads();
+    if (t < 32) {
+      tc5_fence_after();
+      tmem_dealloc(tbase, 32 * CT::NWG);
+    }
+  }
 }
 
 // The pipelined variant: the tile lives in registers while it computes, so
@@ -271,16 +344,16 @@ static int coltma_map(CUtensorMap* m, const void* base, int esz, const PassDesc&
 int launch_coltma(const PassDesc& d, int elem_bytes, int b2, long long grid, int threads,
                          size_t smem, void* stream) {
   int seen = 0;  // candidates of this geometry so far; d.tma - 1 picks one
-#define PAC_X(T, BY, B2_, MO, SG, LL, LW, NT_, MB, PP, DF)                                      \
+#define PAC_X(T, BY, B2_, MO, SG, LL, LW, NT_, MB, PP, DF, TC_)                                   \
   if (elem_bytes == BY && b2 == B2_ && d.mode == MO && d.sign == SG && d.logL == LL &&     \
-      seen++ == d.tma - 1) {                                                               \
+      d.tc == TC_ && seen++ == d.tma - 1) {                                                \
     using CT = ColTma<T, B2_, MO, SG, LL, LW, NT_>;                                        \
     if (d.W != (1 << LW) || threads != NT_)                                                \
       return set_error(PAC_ERROR_INTERNAL, "tensor-copy column pass geometry mismatch");   \
     static std::mutex mu;                                                                  \
     static std::set<int> configured;                                                       \
     auto kern = PP ? pac_coltma_pipe_kernel<T, B2_, MO, SG, LL, LW, NT_, MB>               \
-                   : pac_coltma_kernel<T, B2_, MO, SG, LL, LW, NT_, MB>;                   \
+                   : pac_coltma_kernel<T, B2_, MO, SG, LL, LW, NT_, MB, TC_>;              \
     CUtensorMap m[4];                                                                      \
     const bool tin = MO == MODE_DIT, tout = MO == MODE_DIF;                                \
     PAC_TRY_BE(coltma_map(&m[0], d.in_re, BY, d, CT::W, CT::BOXR, tin, CT::VIN, CT::BOXB)); \

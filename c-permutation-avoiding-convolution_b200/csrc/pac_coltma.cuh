@@ -51,7 +51,7 @@ namespace pac {
 
 enum { LAY_DENSE = 0, LAY_TRANS = 1, LAY_SWZ = 2 };
 
-template <typename T, int B2, int MODE, int SIGN, int LOGL, int LOGW, int NT>
+template <typename T, int B2, int MODE, int SIGN, int LOGL, int LOGW, int NT, int TC = 0>
 struct ColTma {
   using RS = RadsFor<LOGL, B2>;
   static constexpr int L = 1 << LOGL;
@@ -223,6 +223,116 @@ struct ColTma {
       });
     });
   }
+
+  // ---- tensor-core radix-16 steps (TC = 1, the FP32 tensor-core form) ----
+  // Every radix-16 butterfly is one row of a real MMA on the 5th-generation
+  // tensor cores (tcgen05.mma kind::f16, FP32 accumulation in tensor
+  // memory): the 128 threads of a warpgroup put their butterflies' inputs
+  // into rows 0..127 of A (M = 128, K = 32: the 16 real parts, then the 16
+  // imaginary parts), B holds the real 32 x 32 form of the 16-point DFT
+  // (N = 32 outputs: 16 real parts, then 16 imaginary parts), and row r of
+  // D -- read back by the thread that wrote row r (tcgen05.ld 32x32b: warp
+  // w of the warpgroup reads lanes 32w..32w+31) -- holds its butterfly's
+  // outputs in the register order dft_reg leaves (register p = frequency
+  // brev(p)).  Each product is compensated as in the warp-MMA form: inputs
+  // scaled by a power of two into [2^14, 2^15), split into FP16 hi and lo
+  // parts, Y = Xlo.Vhi + Xhi.Vlo + Xhi.Vhi (small products first).  Operand
+  // tiles sit in shared memory K-major without swizzle: core matrices of 8
+  // rows x 8 halves (16 bytes a row, 128 bytes each), core matrix
+  // (row/8, k/8) at ((row/8) * 4 + k/8) * 128 bytes.
+  static constexpr int UM = 128, UK = 32, UN = 32;
+  static constexpr int NWG = NT / 128;   // warpgroups
+  static constexpr int TPW = TPT / 16;   // radix-16 butterflies of a thread per step
+  static constexpr int UTILE = UM * UK;  // halves of one operand tile (8 KB)
+  static_assert(!TC || (sizeof(T) == 4 && NT % 128 == 0), "tensor-core steps: FP32, warpgroups");
+  static PAC_HDC int umma_off(int row, int k) {
+    return ((((row >> 3) << 2) + (k >> 3)) << 6) + ((row & 7) << 3) + (k & 7);
+  }
+  // the DFT operand (hi and lo halves of Vt[n][k], n-major rows, K
+  // contiguous), words of two halves at umma_off(n, k) / 2 for even k
+  static PAC_HD void tc_fill_v(int idx, uint32_t* Vh, uint32_t* Vl) {
+    const int n = idx >> 4, k = (idx & 15) << 1;  // 32 rows x 16 words
+    float v[2];
+    for (int e = 0; e < 2; ++e) {
+      const int kk = k + e;
+      const int c = n & 15, m = kk & 15;
+      const int f = brev_c(c, 4);
+      float cr, ci;
+      tc_cs16((m * f) & 15, cr, ci);
+      if (SIGN < 0) ci = -ci;
+      // Re y_c = sum xr cr - xi ci ; Im y_c = sum xr ci + xi cr
+      v[e] = n < 16 ? (kk < 16 ? cr : -ci) : (kk < 16 ? ci : cr);
+    }
+    uint32_t hi, lo;
+    tc_split2(v[0], v[1], hi, lo);
+    Vh[umma_off(n, k) >> 1] = hi;
+    Vl[umma_off(n, k) >> 1] = lo;
+  }
+  // step S, radix-16 butterfly kk of thread t: DIT pre-twiddles, scale, and
+  // the hi / lo rows (row t mod 128) of this warpgroup's A tiles
+  template <int S>
+  static PAC_HD void tc_prep(const PassDesc& d, int t, int kk, const Cx<T> (&x)[TPT], uint32_t* Ah,
+                             uint32_t* Al, int& E) {
+    constexpr int I = stage_at(S);
+    constexpr int logell = RS::logK(LOGL, I) - 4;
+    static_assert(RS::v[I] == 4, "radix-16 steps only");
+    int w, e0, j;
+    coords<I>(t, kk, w, e0, j);
+    Cx<T> y[16];
+    static_for<16>([&](auto mm) { y[mm.value] = x[kk * 16 + mm.value]; });
+    if constexpr (!DIF) {
+      if (logell > 0 && j > 0) {
+        Cx<T> wv[16];
+        stage_twiddles<T, 16>((const Cx<T>*)d.tw + d.tw_off[I] + j, 1 << logell, wv);
+        static_for<15>([&](auto ss) { y[ss.value + 1] = ctw(y[ss.value + 1], wv[ss.value + 1], SIGN); });
+      }
+    }
+    float mx = 0.f;
+    static_for<16>([&](auto mm) {
+      mx = fmaxf(mx, fmaxf(fabsf(y[mm.value].re), fabsf(y[mm.value].im)));
+    });
+    const int ex = (int)((f32_bits(mx) >> 23) & 0xffu) - 127;  // -127 for 0 / subnormal
+    E = 14 - ex;
+    E = E < -100 ? -100 : E > 100 ? 100 : E;
+    const float sc = tc_pow2(E);
+    const int r = t & 127;
+    static_for<8>([&](auto pp) {  // words of k = 2p, 2p + 1 (real parts) and 16 + 2p, 17 + 2p
+      constexpr int p2 = 2 * pp.value;
+      uint32_t hi, lo;
+      tc_split2(y[p2].re * sc, y[p2 + 1].re * sc, hi, lo);
+      Ah[umma_off(r, p2) >> 1] = hi;
+      Al[umma_off(r, p2) >> 1] = lo;
+      tc_split2(y[p2].im * sc, y[p2 + 1].im * sc, hi, lo);
+      Ah[umma_off(r, 16 + p2) >> 1] = hi;
+      Al[umma_off(r, 16 + p2) >> 1] = lo;
+    });
+  }
+  // step S, radix-16 butterfly kk of thread t: D row (32 floats) unscaled,
+  // DIF post-twiddles, back into x
+  template <int S>
+  static PAC_HD void tc_finish(const PassDesc& d, int t, int kk, const float (&D)[32], int E,
+                               Cx<T> (&x)[TPT]) {
+    constexpr int I = stage_at(S);
+    constexpr int logell = RS::logK(LOGL, I) - 4;
+    int w, e0, j;
+    coords<I>(t, kk, w, e0, j);
+    const float us = tc_pow2(-E);
+    Cx<T> y[16];
+    static_for<16>([&](auto pp) { y[pp.value] = Cx<T>{D[pp.value] * us, D[16 + pp.value] * us}; });
+    if constexpr (DIF) {
+      if (logell > 0 && j > 0) {
+        Cx<T> wv[16];
+        stage_twiddles<T, 16>((const Cx<T>*)d.tw + d.tw_off[I] + j, 1 << logell, wv);
+        static_for<16>([&](auto pp) {
+          constexpr int s = brev_c(pp.value, 4);
+          if constexpr (s > 0) y[pp.value] = ctw(y[pp.value], wv[s], SIGN);
+        });
+      }
+    }
+    static_for<16>([&](auto pp) { x[kk * 16 + pp.value] = y[pp.value]; });
+  }
+  // does step S run on the tensor cores?
+  static PAC_HDC bool tc_step(int s) { return TC && RS::v[stage_at(s)] == 4; }
 
   // tile -> tensor coordinates: column i0 of the row array, outer index o
   static PAC_HD void tile_coords(const PassDesc& d, long long tile, int& i0, int& o) {

@@ -215,9 +215,36 @@ static void replay_cluster(const PassDesc& d, long long grid) {
 // writes for all threads in turn -- the order the kernel's barriers impose.
 // The buffer starts every tile as NaN, so a read of a slot that no copy or
 // stage wrote shows up in the results.
-template <typename T, int B2, int MODE, int SIGN, int LOGL, int LOGW, int NT, int PIPE>
+// Host model of the tensor-core step's MMA for one warpgroup: D = Xlo.Vhi +
+// Xhi.Vlo + Xhi.Vhi over the operand tiles (FP16 halves in the K-major core-
+// matrix layout), each product summed over K in FP64 and the three sums
+// added in FP32 in that order.
+template <class CT>
+static void tc_mma_warpgroup(const uint32_t* Ah, const uint32_t* Al, const uint32_t* Vh,
+                             const uint32_t* Vl, float (*D)[32]) {
+  auto half = [](const uint32_t* m, int row, int k) {
+    const uint32_t w = m[CT::umma_off(row, k) >> 1];
+    float lo, hi;
+    tc_unpack(w, lo, hi);
+    return (k & 1) ? hi : lo;
+  };
+  for (int r = 0; r < CT::UM; ++r)
+    for (int n = 0; n < CT::UN; ++n) {
+      double p[3] = {0.0, 0.0, 0.0};
+      for (int k = 0; k < CT::UK; ++k) {
+        const double ah = half(Ah, r, k), al = half(Al, r, k);
+        const double vh = half(Vh, n, k), vl = half(Vl, n, k);
+        p[0] += al * vh;
+        p[1] += ah * vl;
+        p[2] += ah * vh;
+      }
+      D[r][n] = ((float)p[0] + (float)p[1]) + (float)p[2];
+    }
+}
+
+template <typename T, int B2, int MODE, int SIGN, int LOGL, int LOGW, int NT, int PIPE, int TC>
 static int replay_coltma(const PassDesc& d, long long grid) {
-  using CT = ColTma<T, B2, MODE, SIGN, LOGL, LOGW, NT>;
+  using CT = ColTma<T, B2, MODE, SIGN, LOGL, LOGW, NT, TC>;
   constexpr int W = CT::W, L = CT::L, NS = CT::NS, TILE = CT::TILE;
   if (copy_wait_gives_up(d)) return PAC_SUCCESS;
   struct Regs {
@@ -287,7 +314,34 @@ static int replay_coltma(const PassDesc& d, long long grid) {
         static_for<NS>([&](auto ss) {
           constexpr int St = ss.value;
           each([&](int t, Cx<T>(&x)[CT::TPT]) { CT::template read<St>(t, Bre, Bim, x); });
-          each([&](int t, Cx<T>(&x)[CT::TPT]) { CT::template compute<St>(d, tile, t, x); });
+          if constexpr (CT::tc_step(St)) {
+            // per warpgroup: every thread's A rows, the MMA, every thread's
+            // D row -- round by round
+            constexpr int NWG = CT::NWG;
+            std::vector<uint32_t> A((size_t)NWG * CT::UTILE), V(1024);
+            for (int i = 0; i < 512; ++i) CT::tc_fill_v(i, V.data(), V.data() + 512);
+            std::vector<int> E(NT);
+            std::vector<float> D((size_t)NWG * CT::UM * 32);
+            static_for<CT::TPW>([&](auto kk) {
+              std::fill(A.begin(), A.end(), 0xffffffffu);  // NaN halves
+              each([&](int t, Cx<T>(&x)[CT::TPT]) {
+                uint32_t* Ah = A.data() + (size_t)(t >> 7) * CT::UTILE;
+                CT::template tc_prep<St>(d, t, kk.value, x, Ah, Ah + CT::UTILE / 2, E[t]);
+              });
+              for (int g = 0; g < NWG; ++g) {
+                const uint32_t* Ah = A.data() + (size_t)g * CT::UTILE;
+                tc_mma_warpgroup<CT>(Ah, Ah + CT::UTILE / 2, V.data(), V.data() + 512,
+                                     (float(*)[32])(D.data() + (size_t)g * CT::UM * 32));
+              }
+              each([&](int t, Cx<T>(&x)[CT::TPT]) {
+                float row[32];
+                for (int c = 0; c < 32; ++c) row[c] = D[(size_t)t * 32 + c];
+                CT::template tc_finish<St>(d, t, kk.value, row, E[t], x);
+              });
+            });
+          } else {
+            each([&](int t, Cx<T>(&x)[CT::TPT]) { CT::template compute<St>(d, tile, t, x); });
+          }
           each([&](int t, Cx<T>(&x)[CT::TPT]) { CT::template write<St>(d, t, Bre, Bim, x); });
         });
       }
@@ -349,11 +403,11 @@ int be_launch_pass(const PassDesc& d, int elem_bytes, int b2, long long grid, in
   }
   if (d.tma) {
     int seen = 0;  // candidates of this geometry so far; d.tma - 1 picks one
-#define PAC_X(T, BY, B2_, MO, SG, LL, LW, NT_, MB, PP, DF)                                      \
+#define PAC_X(T, BY, B2_, MO, SG, LL, LW, NT_, MB, PP, DF, TC_)                                   \
   if (elem_bytes == BY && b2 == B2_ && d.mode == MO && d.sign == SG && d.logL == LL &&     \
-      seen++ == d.tma - 1 && d.W == (1 << LW) && threads == NT_) {                         \
+      d.tc == TC_ && seen++ == d.tma - 1 && d.W == (1 << LW) && threads == NT_) {          \
     g_launches++;                                                                          \
-    return replay_coltma<T, B2_, MO, SG, LL, LW, NT_, PP>(d, grid);                        \
+    return replay_coltma<T, B2_, MO, SG, LL, LW, NT_, PP, TC_>(d, grid);                   \
   }
     PAC_COLTMA_LIST(PAC_X)
 #undef PAC_X

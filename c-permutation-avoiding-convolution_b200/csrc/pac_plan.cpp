@@ -426,11 +426,11 @@ static void apply_special(const Schedule& s, PassSpec& p) {
   // Plain DIF / DIT passes of the default radix schedule, 16-byte aligned
   // arrays; not with specialised kernels tuned off.
   const char* tv = getenv("PAC_COLTMA");
-  const int tvar = (d.tc || s.rlog_cap < 4 || s.special < 0) ? 0 : tv ? atoi(tv) : -1;
+  const int tvar = (s.rlog_cap < 4 || s.special < 0) ? 0 : tv ? atoi(tv) : -1;
   int tminb = 1, tpipe = 0, tcand = 0;
   if (d.logS > 0 && cvar == nullptr && tvar != 0 && d.tw4 == 0 &&
       (d.mode == MODE_DIF || d.mode == MODE_DIT) &&
-      coltma_geometry(s.bytes, p.b2, d.mode, d.sign, d.logL, &logW, &nt, &tminb, &tpipe,
+      coltma_geometry(s.bytes, p.b2, d.mode, d.sign, d.logL, d.tc, &logW, &nt, &tminb, &tpipe,
                       tvar > 0 ? tvar - 1 : -1, &tcand) &&
       rads_match(d, d.logL, p.b2, 4) && logW <= d.logS &&
       (d.nlines & ((1LL << logW) - 1)) == 0 && (d.nlines >> d.logS) < (1LL << 31) &&
@@ -446,6 +446,9 @@ static void apply_special(const Schedule& s, PassSpec& p) {
     p.threads = nt;
     p.grid = tiles < slots ? tiles : slots;
     p.smem = (size_t)(tpipe ? 3 : 2) * d.W * d.L * s.bytes + 1024;
+    // tensor-core form: per warpgroup two 8 KB operand tiles, and the DFT
+    // operand's two 2 KB tiles
+    if (d.tc) p.smem += (size_t)(nt / 128) * 16384 + 4096;
     return;
   }
   const char* var = getenv("PAC_SPECIAL_VARIANT");

@@ -74,8 +74,8 @@ PAC_HD void plane_xstage(const PassDesc& d, long long plane, const ClView<T, G::
   static_for<R>([&](auto mm) {
     constexpr int m = mm.value;
     constexpr int slot = DIF ? m : drev_c(m, LR, B2);
-    const int row = j + (slot << logell);
     if constexpr (DIF) {
+      const int row = j + (slot << logell);
       const long long gi = base + ((long long)row << G::kLogN2) + col;
       x[m] = Cx<T>{ld_g((const T*)d.in_re + gi), ld_g((const T*)d.in_im + gi)};
     } else {
@@ -90,7 +90,6 @@ PAC_HD void plane_xstage(const PassDesc& d, long long plane, const ClView<T, G::
   static_for<R>([&](auto pp) {
     constexpr int p = pp.value;
     constexpr int slot = DIF ? drev_c(brev_c(p, LR), LR, B2) : brev_c(p, LR);
-    const int row = j + (slot << logell);
     if constexpr (DIF) {
       constexpr int o = (slot << logell) >> G::LOGRC;
       constexpr int roff = (slot << logell) & (G::RC - 1);
@@ -98,6 +97,7 @@ PAC_HD void plane_xstage(const PassDesc& d, long long plane, const ClView<T, G::
       cv.re[o][si] = x[p].re;
       cv.im[o][si] = x[p].im;
     } else {
+      const int row = j + (slot << logell);
       const long long gi = base + ((long long)row << G::kLogN2) + col;
       ((T*)d.out_re)[gi] = x[p].re;
       ((T*)d.out_im)[gi] = x[p].im;

@@ -136,31 +136,34 @@ namespace pac {
 // FP32 passes keep the load/store-unit kernel.
 // fields: element type, bytes, log2 digit base, mode, sign, log2 L, log2 W,
 // threads, CTAs per SM, pipelined, default
-#define PAC_COLTMA_LIST(X)                                 \
-  X(double, 8, 1, MODE_DIF, -1, 11, 2, 512, 1, 0, 0)       \
-  X(double, 8, 1, MODE_DIT, +1, 11, 2, 512, 1, 0, 0)       \
-  X(float, 4, 1, MODE_DIF, -1, 11, 3, 512, 1, 0, 0)        \
-  X(float, 4, 1, MODE_DIT, +1, 11, 3, 512, 1, 0, 0)        \
-  X(double, 8, 1, MODE_DIF, -1, 11, 1, 256, 2, 0, 0)       \
-  X(double, 8, 1, MODE_DIT, +1, 11, 1, 256, 2, 0, 0)       \
-  X(float, 4, 1, MODE_DIF, -1, 11, 2, 256, 2, 0, 0)        \
-  X(float, 4, 1, MODE_DIT, +1, 11, 2, 256, 2, 0, 0)        \
-  X(double, 8, 1, MODE_DIF, -1, 11, 2, 512, 1, 1, 1)       \
-  X(double, 8, 1, MODE_DIT, +1, 11, 2, 512, 1, 1, 1)       \
-  X(float, 4, 1, MODE_DIF, -1, 11, 3, 512, 1, 1, 0)        \
-  X(float, 4, 1, MODE_DIT, +1, 11, 3, 512, 1, 1, 0)        \
-  X(float, 4, 1, MODE_DIF, -1, 11, 3, 1024, 1, 1, 0)       \
-  X(float, 4, 1, MODE_DIT, +1, 11, 3, 1024, 1, 1, 0)       \
-  X(float, 4, 1, MODE_DIF, -1, 11, 3, 1024, 1, 0, 0)       \
-  X(float, 4, 1, MODE_DIT, +1, 11, 3, 1024, 1, 0, 0)
+#define PAC_COLTMA_LIST(X)                                     \
+  X(double, 8, 1, MODE_DIF, -1, 11, 2, 512, 1, 0, 0, 0)        \
+  X(double, 8, 1, MODE_DIT, +1, 11, 2, 512, 1, 0, 0, 0)        \
+  X(float, 4, 1, MODE_DIF, -1, 11, 3, 512, 1, 0, 0, 0)         \
+  X(float, 4, 1, MODE_DIT, +1, 11, 3, 512, 1, 0, 0, 0)         \
+  X(double, 8, 1, MODE_DIF, -1, 11, 1, 256, 2, 0, 0, 0)        \
+  X(double, 8, 1, MODE_DIT, +1, 11, 1, 256, 2, 0, 0, 0)        \
+  X(float, 4, 1, MODE_DIF, -1, 11, 2, 256, 2, 0, 0, 0)         \
+  X(float, 4, 1, MODE_DIT, +1, 11, 2, 256, 2, 0, 0, 0)         \
+  X(double, 8, 1, MODE_DIF, -1, 11, 2, 512, 1, 1, 1, 0)        \
+  X(double, 8, 1, MODE_DIT, +1, 11, 2, 512, 1, 1, 1, 0)        \
+  X(float, 4, 1, MODE_DIF, -1, 11, 3, 512, 1, 1, 0, 0)         \
+  X(float, 4, 1, MODE_DIT, +1, 11, 3, 512, 1, 1, 0, 0)         \
+  X(float, 4, 1, MODE_DIF, -1, 11, 3, 1024, 1, 1, 0, 0)        \
+  X(float, 4, 1, MODE_DIT, +1, 11, 3, 1024, 1, 1, 0, 0)        \
+  X(float, 4, 1, MODE_DIF, -1, 11, 3, 1024, 1, 0, 0, 0)        \
+  X(float, 4, 1, MODE_DIT, +1, 11, 3, 1024, 1, 0, 0, 0)        \
+  /* tensor-core form: radix-16 steps on tcgen05 MMAs */         \
+  X(float, 4, 1, MODE_DIF, -1, 11, 3, 512, 1, 0, 0, 1)         \
+  X(float, 4, 1, MODE_DIT, +1, 11, 3, 512, 1, 0, 0, 1)
 
 // the variant-th candidate of a geometry (variant < 0: its default entry);
 // *cand returns its 1-based candidate number
-inline bool coltma_geometry(int bytes, int b2, int mode, int sign, int logL, int* logW, int* nt,
-                            int* minb, int* pipe, int variant, int* cand) {
+inline bool coltma_geometry(int bytes, int b2, int mode, int sign, int logL, int tc, int* logW,
+                            int* nt, int* minb, int* pipe, int variant, int* cand) {
   int seen = 0;
-#define PAC_X(T, BY, B2_, MO, SG, LL, LW, NT_, MB, PP, DF)                                \
-  if (bytes == BY && b2 == B2_ && mode == MO && sign == SG && logL == LL &&            \
+#define PAC_X(T, BY, B2_, MO, SG, LL, LW, NT_, MB, PP, DF, TC_)                           \
+  if (bytes == BY && b2 == B2_ && mode == MO && sign == SG && logL == LL && tc == TC_ && \
       (variant < 0 ? (++seen, DF == 1) : seen++ == variant)) {                         \
     *logW = LW;                                                                        \
     *nt = NT_;                                                                         \

@@ -177,6 +177,16 @@ def test_column_kernels(emu, orc, monkeypatch, form, kind):
     P.check_column_kernels(emu, orc, (2048, 32), 2, form, monkeypatch, kind)
 
 
+@pytest.mark.parametrize("dims,batch", [((2048, 32), 2), ((2048, 8), 1)])
+def test_tc_tcgen05_columns(emu, orc, monkeypatch, dims, batch):
+    """Tensor-core form with the column passes' radix-16 steps on tcgen05
+    MMAs (PAC_COLTMA=1 picks the tensor-copy kernel's tensor-core variant):
+    the replay of the A rows, the MMA (modelled from the FP16 halves) and
+    the D rows against numpy and the oracle."""
+    monkeypatch.setenv("PAC_COLTMA", "1")
+    P.check_tc(emu, orc, dims, batch, 2, ops=True)
+
+
 @pytest.mark.parametrize("dims,batch,form,per", [((2, 256, 256), 1, 1, False),
                                                   ((2, 256, 128), 2, 1, True),
                                                   ((2, 256, 256), 1, 0, False),

@@ -234,6 +234,16 @@ def test_column_kernels(lib, orc, monkeypatch, form, kind):
 
 
 
+@pytest.mark.parametrize("dims,batch", [((2048, 32), 2), ((2048, 256), 1), ((2048, 2048), 1)])
+def test_tc_tcgen05_columns(lib, orc, monkeypatch, dims, batch):
+    """Tensor-core form with the column passes' radix-16 steps on tcgen05
+    MMAs (tensor memory accumulators, operands in shared memory, one MMA of
+    M = 128 butterflies per warpgroup and round) against numpy's FP64 FFT
+    convolution and the oracle's butterflies, within the form's tolerance."""
+    monkeypatch.setenv("PAC_COLTMA", "1")
+    P.check_tc(lib, orc, dims, batch, 2, ops=dims[1] <= 256)
+
+
 @pytest.mark.parametrize("dims,batch,form,per", [((256, 256, 256), 1, 1, False),
                                                   ((512, 256, 128), 1, 1, False),
                                                   ((8, 256, 256), 3, 1, True),

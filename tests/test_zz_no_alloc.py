@@ -64,5 +64,11 @@ def test_noalloc_rejects_oversize(lib):
         assert np.all(d.get(y, (n,), np.float64) == 7.0)
         st = lib.pac_convolve_1d_noalloc(ptrs[0], ptrs[1], ptrs[2], ptrs[3], y, y, 96, 1, None)
         assert st == 2  # not a power of 2
+        # sizes near the int range are rejected by the limit before any shift
+        for big in ((1 << 30) + 1, 1 << 30, 2147483647):
+            st = lib.pac_convolve_1d_noalloc(ptrs[0], ptrs[1], ptrs[2], ptrs[3], y, y, big, 1,
+                                             None)
+            assert st == 4
+        assert np.all(d.get(y, (n,), np.float64) == 7.0)
     finally:
         d.free()
