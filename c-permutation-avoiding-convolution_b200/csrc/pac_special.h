@@ -49,7 +49,8 @@ namespace pac {
   /* the fused 2048-point FP32 pass at three and two CTAs per SM; on */      \
   /* 2048^2 four (64 registers, no spills) ran 33.2 us, three 34.9, two */   \
   /* 37.2; the FP64 pass at five CTAs per SM spills 144 bytes and ran */    \
-  /* 53.2 us against 47.2 at four */                                          \
+  /* 53.2 us against 47.2 at four, and with two lines per 256-thread CTA */  \
+  /* (two CTAs per SM) 51.4 against 46.5 */                                  \
   X(float, 4, 1, MODE_CONV, 0, 11, 0, 1, 256, 3, 0, 4)           \
   X(float, 4, 1, MODE_CONV, 0, 11, 0, 1, 256, 2, 0, 4)           \
   /* the 3D passes at the other occupancy: on 512 x 256 x 128 the */     \
