@@ -64,14 +64,19 @@ CONFIGS = {
 }
 
 # DRAM bytes per convolution (dram__bytes_read.sum + dram__bytes_write.sum
-# summed over its three passes) from one ncu capture of the same workload and
-# kernels (command in TRAFFIC_SOURCE).  ncu flushes L2 between kernels, so
+# summed over its three passes, mean of the 6 convolutions of the run) from
+# one ncu capture of the same workload and default kernels (command in
+# TRAFFIC_SOURCE, FORM = f64 / f32 / tc).  ncu flushes L2 between kernels, so
 # these are cold-cache figures: reads equal the algorithmic reads of every
-# pass; the timed runs keep the output L2-persisting, so their own DRAM bytes
-# can only be lower.
+# pass, and part of every pass's write-back happens after the kernel ends;
+# the timed runs keep the output L2-persisting, so their own DRAM bytes can
+# only be lower.
 FORMS = {"f64": pac.PAC_FORM_F64, "f32": pac.PAC_FORM_F32, "tc": pac.PAC_FORM_TC}
-MEASURED_TRAFFIC = {("c3", "f64"): 337652480, ("c3", "f32"): 137554432,
-                    ("c3", "tc"): 136706304}
+MEASURED_TRAFFIC = {("c3", "f64"): 317809237, ("c3", "f32"): 134629717,
+                    ("c3", "tc"): 134536661}
+TRAFFIC_SOURCE = ("ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,"
+                  "gpu__time_duration.sum --clock-control none --csv python bench.py "
+                  "--profile --config c3 --form FORM --tune off --steps 3 --warmup 3")
 
 
 def make_inputs(cfg_name, batch=None):
@@ -400,6 +405,8 @@ def run_ours(args, world, dist):
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4),
                 "traffic": MEASURED_TRAFFIC.get((args.config, args.form)),
+                "traffic_source": TRAFFIC_SOURCE if (args.config, args.form) in MEASURED_TRAFFIC
+                else None,
                 "peak_source": "measured, MEASURED_PEAKS.json hbm_gbs" if peak_kind == "measured"
                 else "fallback 6650 GB/s",
                 "kernel": f"pac_pass_kernel x{len(pass_ms)} = one convolution",

@@ -202,9 +202,13 @@ __global__ void __launch_bounds__(NT, MINB)
 // then -- the load runs under this tile's arithmetic.  The stages exchange
 // through X, a buffer of one component in the swizzled layout (real parts,
 // then imaginary parts), and each component of the result leaves by a
-// tensor store from X (transposed view for DIF, dense rows for DIT).
-// Shared memory: A (both components) + X.  Waits bounded as above.
-template <typename T, int B2, int MODE, int SIGN, int LOGL, int LOGW, int NT, int MINB>
+// tensor store from X (transposed view for DIF, dense rows for DIT).  With
+// GST the result leaves the registers by plain stores instead (ColTma::
+// store_g), so the tensor-copy unit carries only the loads and the last step
+// needs no exchange.  Shared memory: A (both components) + X.  Waits bounded
+// as above.
+template <typename T, int B2, int MODE, int SIGN, int LOGL, int LOGW, int NT, int MINB,
+          bool GST>
 __global__ void __launch_bounds__(NT, MINB)
     pac_coltma_pipe_kernel(const PassDesc d, const __grid_constant__ CUtensorMap tin_re,
                            const __grid_constant__ CUtensorMap tin_im,
@@ -219,6 +223,7 @@ __global__ void __launch_bounds__(NT, MINB)
   T* Are = reinterpret_cast<T*>(((uintptr_t)pac_smem_raw + 1023) & ~(uintptr_t)1023);
   T* Aim = Are + TILE;
   T* X = Aim + TILE;
+  Cx<T>* tws = reinterpret_cast<Cx<T>*>(X + TILE);  // the stage twiddles (CT::TWSM)
   const int t = threadIdx.x;
   const long long ntiles = d.nlines >> LOGW;
   auto issue_load = [&](long long tl) {
@@ -253,6 +258,7 @@ __global__ void __launch_bounds__(NT, MINB)
     mbar_init(&bar, 1);
     fence_barrier_init();
   }
+  CT::tw_fill(d, t, tws);
   __syncthreads();
   long long tile = blockIdx.x;
   if (t == 0 && tile < ntiles) issue_load(tile);
@@ -274,7 +280,7 @@ __global__ void __launch_bounds__(NT, MINB)
     if (t == 0 && tile + gridDim.x < ntiles) issue_load(tile + gridDim.x);
     static_for<NS>([&](auto ss) {
       constexpr int S = ss.value;
-      CT::template compute<S>(d, tile, t, x);
+      CT::template compute<S>(d, tile, t, x, tws);
       if constexpr (S < NS - 1) {
         CT::template write_c<S, 0, LAY_SWZ>(d, t, X, x);
         __syncthreads();
@@ -286,20 +292,24 @@ __global__ void __launch_bounds__(NT, MINB)
         __syncthreads();
       }
     });
-    CT::template write_c<NS - 1, 0, LOUT>(d, t, X, x);
-    fence_proxy_async();
-    __syncthreads();
-    if (t == 0) {
-      issue_store(&tout_re, tile);
-      bulk_wait_read();
-    }
-    __syncthreads();
-    CT::template write_c<NS - 1, 1, LOUT>(d, t, X, x);
-    fence_proxy_async();
-    __syncthreads();
-    if (t == 0) {
-      issue_store(&tout_im, tile);
-      bulk_wait_read();
+    if constexpr (GST) {
+      CT::template store_g<NS - 1>(d, tile, t, x);
+    } else {
+      CT::template write_c<NS - 1, 0, LOUT>(d, t, X, x);
+      fence_proxy_async();
+      __syncthreads();
+      if (t == 0) {
+        issue_store(&tout_re, tile);
+        bulk_wait_read();
+      }
+      __syncthreads();
+      CT::template write_c<NS - 1, 1, LOUT>(d, t, X, x);
+      fence_proxy_async();
+      __syncthreads();
+      if (t == 0) {
+        issue_store(&tout_im, tile);
+        bulk_wait_read();
+      }
     }
   }
   if (t == 0) bulk_wait_all();
@@ -352,7 +362,9 @@ int launch_coltma(const PassDesc& d, int elem_bytes, int b2, long long grid, int
       return set_error(PAC_ERROR_INTERNAL, "tensor-copy column pass geometry mismatch");   \
     static std::mutex mu;                                                                  \
     static std::set<int> configured;                                                       \
-    auto kern = PP ? pac_coltma_pipe_kernel<T, B2_, MO, SG, LL, LW, NT_, MB>               \
+    /* the pipelined kernel keeps a copy of the stage twiddles after its buffers */        \
+    const size_t sm = smem + (PP ? (size_t)CT::TWSM * 2 * sizeof(T) : 0);                  \
+    auto kern = PP ? pac_coltma_pipe_kernel<T, B2_, MO, SG, LL, LW, NT_, MB, PP == 2>      \
                    : pac_coltma_kernel<T, B2_, MO, SG, LL, LW, NT_, MB, TC_>;              \
     CUtensorMap m[4];                                                                      \
     const bool tin = MO == MODE_DIT, tout = MO == MODE_DIF;                                \
@@ -366,13 +378,13 @@ int launch_coltma(const PassDesc& d, int elem_bytes, int b2, long long grid, int
       std::lock_guard<std::mutex> g(mu);                                                   \
       if (!configured.count(dev)) {                                                        \
         PAC_CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,     \
-                                    (int)smem),                                            \
+                                    (int)sm),                                              \
                "cudaFuncSetAttribute");                                                    \
         configured.insert(dev);                                                            \
       }                                                                                    \
     }                                                                                      \
     if (grid > 0x7fffffffLL) return set_error(PAC_ERROR_SIZE, "pass grid too large");      \
-    kern<<<(unsigned)grid, threads, smem, (cudaStream_t)stream>>>(d, m[0], m[1], m[2], m[3]); \
+    kern<<<(unsigned)grid, threads, sm, (cudaStream_t)stream>>>(d, m[0], m[1], m[2], m[3]); \
     PAC_CU(cudaGetLastError(), "pac_coltma_kernel launch");                                \
     count_launch();                                    \
     return PAC_SUCCESS;                                                                    \

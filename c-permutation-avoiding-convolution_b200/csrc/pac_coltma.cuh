@@ -141,18 +141,59 @@ struct ColTma {
     });
   }
 
-  // step S, part 2: the butterflies' arithmetic on the registers
+  // ---- stage twiddles in shared memory (the pipelined variant) ----------
+  // Every tile of a pass reads the same stage-table entries, so a persistent
+  // CTA copies the rows that the butterflies read once, at its start, and
+  // the stages read them from shared memory: for stage I with ell > 1, rows
+  // r < tw_rows(I) of ell entries, row r = table row tw_s(I, r) - 1
+  // (stage_twiddles_c's layout).  2048-point FP64: 544 entries (8.5 KB).
+  static PAC_HDC int tw_ell(int I) { return 1 << (RS::logK(LOGL, I) - RS::v[I]); }
+  static PAC_HDC int tw_rows(int I) {
+    return (sizeof(T) == 8 && RS::v[I] >= 2) ? RS::v[I] : (1 << RS::v[I]) - 1;
+  }
+  static PAC_HDC int tw_s(int I, int r) {
+    return (sizeof(T) == 8 && RS::v[I] >= 2) ? 1 << r : r + 1;
+  }
+  static PAC_HDC int tw_base(int I) {
+    int o = 0;
+    for (int i = 0; i < I; ++i)
+      if (tw_ell(i) > 1) o += tw_rows(i) * tw_ell(i);
+    return o;
+  }
+  static constexpr int TWSM = tw_base(NS);  // entries
+  // thread t's share of the copy
+  static PAC_HD void tw_fill(const PassDesc& d, int t, Cx<T>* tws) {
+    static_for<NS>([&](auto ii) {
+      constexpr int I = ii.value;
+      constexpr int ell = tw_ell(I), n = tw_rows(I) * ell;
+      if constexpr (ell > 1) {
+        constexpr int base = tw_base(I);
+        const Cx<T>* src = (const Cx<T>*)d.tw + d.tw_off[I];
+        for (int q = t; q < n; q += NT) {
+          const int r = q / ell, j = q - r * ell;
+          constexpr bool pow2 = tw_s(I, 2) == 4;  // rows of s = 2^r
+          tws[base + q] = src[((pow2 ? 1 << r : r + 1) - 1) * ell + j];
+        }
+      }
+    });
+  }
+
+  // step S, part 2: the butterflies' arithmetic on the registers (stage
+  // twiddles from tws, the shared-memory copy, when given)
   template <int S>
-  static PAC_HD void compute(const PassDesc& d, long long tile, int t, Cx<T> (&x)[TPT]) {
+  static PAC_HD void compute(const PassDesc& d, long long tile, int t, Cx<T> (&x)[TPT],
+                             const Cx<T>* tws = nullptr) {
     constexpr int I = stage_at(S);
     constexpr int LR = RS::v[I], R = 1 << LR;
     constexpr int logell = RS::logK(LOGL, I) - LR;
+    constexpr int tb = tw_base(I);
+    const Cx<T>* twi = tws ? tws + tb : nullptr;
     static_for<TPT / R>([&](auto kk) {
       int w, e0, j;
       coords<I>(t, kk.value, w, e0, j);
       Cx<T> y[R];
       static_for<R>([&](auto mm) { y[mm.value] = x[kk.value * R + mm.value]; });
-      bf_math<T, B2, R, SIGN, DIF, SP>(d, tile, y, w, e0, j, logell, d.tw_off[I]);
+      bf_math<T, B2, R, SIGN, DIF, SP>(d, tile, y, w, e0, j, logell, d.tw_off[I], twi);
       static_for<R>([&](auto mm) { x[kk.value * R + mm.value] = y[mm.value]; });
     });
   }
@@ -220,6 +261,40 @@ struct ColTma {
         T v = C == 0 ? x[kk.value * R + p].re : x[kk.value * R + p].im;
         if (scale) v *= sc;
         B[pos<LAY>(e0 + (out_slot<LR, p>() << logell), w)] = v;
+      });
+    });
+  }
+
+  // the last step's outputs straight from the registers to the pass's output
+  // rows (the pipelined variant's direct-store form): four (FP64) or eight
+  // (FP32) consecutive lanes hold the W columns of one row, so every warp
+  // store fills eight whole 32-byte sectors and the tensor-copy unit only
+  // carries the loads
+  template <int S>
+  static PAC_HD void store_g(const PassDesc& d, long long tile, int t, const Cx<T> (&x)[TPT]) {
+    constexpr int I = stage_at(S);
+    constexpr int LR = RS::v[I], R = 1 << LR;
+    constexpr int logell = RS::logK(LOGL, I) - LR;
+    const bool scale = d.use_scale;
+    const T sc = T(d.scale);
+    int i0, o;
+    tile_coords(d, tile, i0, o);
+    const long long base = ((long long)o << (LOGL + d.logS)) + i0;
+    T* ore = (T*)d.out_re;
+    T* oim = (T*)d.out_im;
+    static_for<TPT / R>([&](auto kk) {
+      int w, e0, j;
+      coords<I>(t, kk.value, w, e0, j);
+      static_for<R>([&](auto pp) {
+        constexpr int p = pp.value;
+        const long long gi = base + ((long long)(e0 + (out_slot<LR, p>() << logell)) << d.logS) + w;
+        Cx<T> v = x[kk.value * R + p];
+        if (scale) {
+          v.re *= sc;
+          v.im *= sc;
+        }
+        ore[gi] = v.re;
+        oim[gi] = v.im;
       });
     });
   }

@@ -296,11 +296,14 @@ static int replay_coltma(const PassDesc& d, long long grid) {
         // the result written into X component by component for the stores
         constexpr int LOUT = CT::DIF ? LAY_TRANS : LAY_DENSE;
         std::vector<T> X((size_t)TILE, std::numeric_limits<T>::quiet_NaN());
+        const T qn = std::numeric_limits<T>::quiet_NaN();
+        std::vector<Cx<T>> tws((size_t)CT::TWSM + 1, Cx<T>{qn, qn});
+        for (int t = 0; t < NT; ++t) CT::tw_fill(d, t, tws.data());
         each([&](int t, Cx<T>(&x)[CT::TPT]) { CT::template read<0>(t, Bre, Bim, x); });
         std::fill(B.begin(), B.end(), std::numeric_limits<T>::quiet_NaN());
         static_for<NS>([&](auto ss) {
           constexpr int St = ss.value;
-          each([&](int t, Cx<T>(&x)[CT::TPT]) { CT::template compute<St>(d, tile, t, x); });
+          each([&](int t, Cx<T>(&x)[CT::TPT]) { CT::template compute<St>(d, tile, t, x, tws.data()); });
           if constexpr (St < NS - 1) {
             each([&](int t, Cx<T>(&x)[CT::TPT]) { CT::template write_c<St, 0, LAY_SWZ>(d, t, X.data(), x); });
             each([&](int t, Cx<T>(&x)[CT::TPT]) { CT::template read_c<St + 1, 0, LAY_SWZ>(t, X.data(), x); });
@@ -308,6 +311,10 @@ static int replay_coltma(const PassDesc& d, long long grid) {
             each([&](int t, Cx<T>(&x)[CT::TPT]) { CT::template read_c<St + 1, 1, LAY_SWZ>(t, X.data(), x); });
           }
         });
+        if constexpr (PIPE == 2) {
+          each([&](int t, Cx<T>(&x)[CT::TPT]) { CT::template store_g<NS - 1>(d, tile, t, x); });
+          continue;
+        }
         each([&](int t, Cx<T>(&x)[CT::TPT]) { CT::template write_c<NS - 1, 0, LOUT>(d, t, Bre, x); });
         each([&](int t, Cx<T>(&x)[CT::TPT]) { CT::template write_c<NS - 1, 1, LOUT>(d, t, Bim, x); });
       } else {

@@ -134,7 +134,12 @@ namespace pac {
 // 54.9 / 51.0 for the load/store-unit kernel (pac_special.h above): the
 // pipelined FP64 variant is the default.  FP32: 36.8 / 32.8, 41.2 / 34.8
 // and 47.4 / 36.9 (the pipelined FP32 tile spills) against 32.0 / 30.1: the
-// FP32 passes keep the load/store-unit kernel.
+// FP32 passes keep the load/store-unit kernel.  The pipelined kernel keeps
+// the stage twiddles in shared memory (ColTma::tw_fill): FP64 DIF 53.1 ->
+// 50.9 us, DIT unchanged at 48.1.  Storing the result from the registers
+// (PP = 2, the tensor-copy unit then carries only the loads) measured
+// 50.7 / 48.1 (FP64) and 34.9 / 30.7 (FP32, 512 threads): no gain, so
+// PP = 2 stays a candidate, not a default.
 // fields: element type, bytes, log2 digit base, mode, sign, log2 L, log2 W,
 // threads, CTAs per SM, pipelined, default
 #define PAC_COLTMA_LIST(X)                                     \
@@ -154,6 +159,13 @@ namespace pac {
   X(float, 4, 1, MODE_DIT, +1, 11, 3, 1024, 1, 1, 0, 0)        \
   X(float, 4, 1, MODE_DIF, -1, 11, 3, 1024, 1, 0, 0, 0)        \
   X(float, 4, 1, MODE_DIT, +1, 11, 3, 1024, 1, 0, 0, 0)        \
+  /* pipelined, the result stored from the registers (PP = 2) */ \
+  X(double, 8, 1, MODE_DIF, -1, 11, 2, 512, 1, 2, 0, 0)        \
+  X(double, 8, 1, MODE_DIT, +1, 11, 2, 512, 1, 2, 0, 0)        \
+  X(float, 4, 1, MODE_DIF, -1, 11, 3, 512, 1, 2, 0, 0)         \
+  X(float, 4, 1, MODE_DIT, +1, 11, 3, 512, 1, 2, 0, 0)         \
+  X(float, 4, 1, MODE_DIF, -1, 11, 3, 1024, 1, 2, 0, 0)        \
+  X(float, 4, 1, MODE_DIT, +1, 11, 3, 1024, 1, 2, 0, 0)        \
   /* tensor-core form: radix-16 steps on tcgen05 MMAs */         \
   X(float, 4, 1, MODE_DIF, -1, 11, 3, 512, 1, 0, 0, 1)         \
   X(float, 4, 1, MODE_DIT, +1, 11, 3, 512, 1, 0, 0, 1)

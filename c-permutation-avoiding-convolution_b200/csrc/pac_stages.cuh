@@ -140,14 +140,36 @@ PAC_HD void stage_twiddles(const Cx<T>* tw, int ell, Cx<T> (&w)[R]) {
   }
 }
 
+// The same twiddles from a compact copy of the table's rows (a CTA's
+// shared-memory copy, see ColTma::tw_fill): row r holds w_K^{j s(r)} for
+// the ell values of j, s(r) = 2^r in FP64 at radix >= 4 (the rows
+// stage_twiddles reads; the other factors are products), else r + 1.
+template <typename T, int R>
+PAC_HD void stage_twiddles_c(const Cx<T>* tws, int ell, Cx<T> (&w)[R]) {
+  if constexpr (sizeof(T) == 8 && R >= 4) {
+    static_for<ilog2(R)>([&](auto b) { w[1 << b.value] = tws[b.value * ell]; });
+    static_for<R>([&](auto ss) {
+      constexpr int s = ss.value;
+      if constexpr (s > 2 && (s & (s - 1)) != 0) {
+        constexpr int hb = 1 << ilog2(s);
+        w[s] = cmul(w[hb], w[s - hb]);
+      }
+    });
+  } else {
+    static_for<R - 1>([&](auto ss) { w[ss.value + 1] = tws[ss.value * ell]; });
+  }
+}
+
 // The arithmetic of one radix-R butterfly on registers x: DIT pre-twiddles,
 // the R-point DFT, DIF post-twiddles.  x[m] holds the element at input slot
 // m (DIF: m, DIT: sigma_b(m)); afterwards register p holds output index
 // brev(p).  e0 is the butterfly's first element, j its index in the block,
-// w its line, ell = 2^logell the element stride.
+// w its line, ell = 2^logell the element stride.  With tws the stage
+// twiddles come from that compact copy of the stage's rows instead of the
+// table in global memory.
 template <typename T, int B2, int R, int SIGN, bool DIF, class SP>
 PAC_HD void bf_math(const PassDesc& d, long long cta, Cx<T> (&x)[R], int w, int e0, int j,
-                    int logell, int twoff) {
+                    int logell, int twoff, const Cx<T>* tws = nullptr) {
   constexpr int LR = ilog2(R);
   const int ell = 1 << logell;
   // stage table, s-major: entry (s-1)*ell + j = w_K^{j s}; for one s the
@@ -164,7 +186,8 @@ PAC_HD void bf_math(const PassDesc& d, long long cta, Cx<T> (&x)[R], int w, int 
     }
     if (twiddle) {
       Cx<T> wv[R];
-      stage_twiddles<T, R>(tw, ell, wv);
+      if (tws) stage_twiddles_c<T, R>(tws + j, ell, wv);
+      else stage_twiddles<T, R>(tw, ell, wv);
       static_for<R - 1>([&](auto ss) {
         constexpr int s = ss.value + 1;
         x[s] = ctw(x[s], wv[s], SIGN);
@@ -176,7 +199,8 @@ PAC_HD void bf_math(const PassDesc& d, long long cta, Cx<T> (&x)[R], int w, int 
   if constexpr (DIF) {
     if (twiddle) {
       Cx<T> wv[R];
-      stage_twiddles<T, R>(tw, ell, wv);
+      if (tws) stage_twiddles_c<T, R>(tws + j, ell, wv);
+      else stage_twiddles<T, R>(tw, ell, wv);
       static_for<R>([&](auto pp) {
         constexpr int s = brev_c(pp.value, LR);
         if constexpr (s > 0) x[pp.value] = ctw(x[pp.value], wv[s], SIGN);

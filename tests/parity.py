@@ -183,7 +183,8 @@ def check_spectrum_orders(L, dims, batch, base, form):
                            rtol=tol, atol=tol * np.abs(pv).max())
 
 
-COLUMN_KERNELS = ("pipe", "tile", "cluster0", "cluster1", "tma1", "tma2", "tma3", "tma4", "tma5")
+COLUMN_KERNELS = ("pipe", "tile", "cluster0", "cluster1", "tma1", "tma2", "tma3", "tma4", "tma5",
+                  "tma6", "tma7")
 
 
 def check_column_kernels(L, orc, dims, batch, form, monkeypatch, kind):
