@@ -108,12 +108,77 @@ def test_c4_3d_f32(lib, shape):
     assert P.crel(y, h) < P.TOL_F32
 
 
-def test_c4_3d_f64_against_oracle(lib, orc):
-    shape = (64, 128, 32)
+@pytest.mark.parametrize("shape", [(64, 128, 32), (256, 256, 256)])
+def test_c4_3d_f64_against_oracle(lib, orc, shape):
+    """C4 in FP64 against the oracle, at full size too (256^3: the oracle
+    takes ~16 s on one core)."""
     x, h = W.c4(shape)
     y = P.native_conv(lib, shape, 1, 2, pac.PAC_FORM_F64, x, h)[0]
     z = orc.convolution(O.METHOD_PAC, 2, x.real, x.imag, h.real, h.imag)
     assert P.crel(y, z[0] + 1j * z[1]) < P.TOL
+
+
+def test_c5_full_batch(lib, orc):
+    """The whole uneven C5 batch (4096 1D and 64 2D problems, 5.5e8
+    elements, FP32 form) in one multi-plan call at full size:
+    - x = delta in every problem gives y = h in every problem, which checks
+      every problem's offsets, levels and plan-order spectrum;
+    - random inputs match the oracle on sampled problems: the longest 1D,
+      the largest 2D and ten drawn at random."""
+    import torch
+
+    dev = torch.device("cuda", 0)
+    shapes = W.c5_shapes()
+    m = pac.MultiPlan(lib, shapes, 2, pac.PAC_FORM_F32)
+    try:
+        off = m.offsets
+        n = int(off[-1])
+        g = torch.Generator(device=dev)
+        g.manual_seed(5)
+        f32 = dict(dtype=torch.float32, device=dev)
+        hr = torch.randn(n, dtype=torch.float64, device=dev, generator=g)
+        hi = torch.randn(n, dtype=torch.float64, device=dev, generator=g)
+        Hr, Hi = torch.empty(n, **f32), torch.empty(n, **f32)
+        m.filter_spectra(hr.data_ptr(), hi.data_ptr(), Hr.data_ptr(), Hi.data_ptr())
+        xr, xi = torch.zeros(n, **f32), torch.zeros(n, **f32)
+        xr[torch.from_numpy(off[:-1]).to(dev)] = 1.0
+        yr, yi = torch.empty(n, **f32), torch.empty(n, **f32)
+        m.convolve(xr.data_ptr(), xi.data_ptr(), Hr.data_ptr(), Hi.data_ptr(), yr.data_ptr(),
+                   yi.data_ptr())
+        torch.cuda.synchronize()
+        # per-problem squared error and norm, by cumulative sums at the offsets
+        ends = torch.from_numpy(off[1:] - 1).to(dev)
+
+        def per_problem(v):
+            c = torch.cumsum(v, 0)[ends]
+            return torch.diff(c, prepend=torch.zeros(1, dtype=c.dtype, device=dev))
+
+        err = per_problem((yr.double() - hr) ** 2 + (yi.double() - hi) ** 2)
+        ref = per_problem(hr ** 2 + hi ** 2)
+        rel = torch.sqrt(err / ref).cpu().numpy()
+        assert rel.shape == (len(shapes),)
+        assert np.all(rel < P.TOL_F32), (int(np.argmax(rel)), float(rel.max()))
+        # random signals, sampled problems against the oracle
+        xr.normal_(generator=g)
+        xi.normal_(generator=g)
+        m.convolve(xr.data_ptr(), xi.data_ptr(), Hr.data_ptr(), Hi.data_ptr(), yr.data_ptr(),
+                   yi.data_ptr())
+        torch.cuda.synchronize()
+        sizes = np.diff(off)
+        one = [p for p, s in enumerate(shapes) if len(s) == 1]
+        two = [p for p, s in enumerate(shapes) if len(s) == 2]
+        pick = {max(one, key=lambda p: sizes[p]), max(two, key=lambda p: sizes[p])}
+        pick |= set(rng(17).choice(len(shapes), 10, replace=False).tolist())
+        for p in sorted(pick):
+            a, b = int(off[p]), int(off[p + 1])
+            seg = lambda t: t[a:b].double().cpu().numpy().reshape(shapes[p])  # noqa: E731
+            x = seg(xr) + 1j * seg(xi)
+            h = seg(hr) + 1j * seg(hi)
+            z = orc.convolution(O.METHOD_PAC, 2, x.real, x.imag, h.real, h.imag)
+            y = seg(yr) + 1j * seg(yi)
+            assert P.crel(y, z[0] + 1j * z[1]) < P.TOL_F32, (p, shapes[p])
+    finally:
+        m.close()
 
 
 @pytest.mark.parametrize("dims,batch,base,form,per", [
