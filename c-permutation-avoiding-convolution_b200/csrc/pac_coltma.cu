@@ -60,7 +60,7 @@ __global__ void __launch_bounds__(NT, MINB)
   __shared__ __align__(8) uint64_t bar;
   __shared__ __align__(8) uint64_t tbar[TC ? CT::NWG : 1];
   __shared__ uint32_t tmem_slot;
-  T* Bre = reinterpret_cast<T*>(((uintptr_t)pac_smem_raw + 1023) & ~(uintptr_t)1023);
+  T* Bre = reinterpret_cast<T*>(smem_align1024(pac_smem_raw));
   T* Bim = Bre + TILE;
   // tensor-core form: per warpgroup the hi and lo A tiles, then the DFT
   // operand's hi and lo tiles (32-bit words of two halves)
@@ -220,7 +220,7 @@ __global__ void __launch_bounds__(NT, MINB)
   constexpr int LOUT = DIF ? LAY_TRANS : LAY_DENSE;
   extern __shared__ unsigned char pac_smem_raw[];
   __shared__ __align__(8) uint64_t bar;
-  T* Are = reinterpret_cast<T*>(((uintptr_t)pac_smem_raw + 1023) & ~(uintptr_t)1023);
+  T* Are = reinterpret_cast<T*>(smem_align1024(pac_smem_raw));
   T* Aim = Are + TILE;
   T* X = Aim + TILE;
   Cx<T>* tws = reinterpret_cast<Cx<T>*>(X + TILE);  // the stage twiddles (CT::TWSM)

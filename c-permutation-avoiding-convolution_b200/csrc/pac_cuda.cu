@@ -202,7 +202,7 @@ __global__ void __launch_bounds__(NT, 1)
   __shared__ long long s_lb[W];
   // dense tile (tensor-copy destination, 1024-byte aligned), then the
   // exchange array
-  T* Are = reinterpret_cast<T*>(((uintptr_t)pac_smem_raw + 1023) & ~(uintptr_t)1023);
+  T* Are = reinterpret_cast<T*>(smem_align1024(pac_smem_raw));
   T* Aim = Are + W * L;
   T* X = Aim + W * L;
   const int t = threadIdx.x;

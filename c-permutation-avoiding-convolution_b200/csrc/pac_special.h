@@ -134,12 +134,15 @@ namespace pac {
 // 54.9 / 51.0 for the load/store-unit kernel (pac_special.h above): the
 // pipelined FP64 variant is the default.  FP32: 36.8 / 32.8, 41.2 / 34.8
 // and 47.4 / 36.9 (the pipelined FP32 tile spills) against 32.0 / 30.1: the
-// FP32 passes keep the load/store-unit kernel.  The pipelined kernel keeps
-// the stage twiddles in shared memory (ColTma::tw_fill): FP64 DIF 53.1 ->
-// 50.9 us, DIT unchanged at 48.1.  Storing the result from the registers
-// (PP = 2, the tensor-copy unit then carries only the loads) measured
-// 50.7 / 48.1 (FP64) and 34.9 / 30.7 (FP32, 512 threads): no gain, so
-// PP = 2 stays a candidate, not a default.
+// FP32 passes kept the load/store-unit kernel.  Then the pipelined kernel
+// took the stage twiddles from shared memory (ColTma::tw_fill): FP64 DIF
+// 53.1 -> 50.9 us, DIT 48.1.  And its tile pointers, rounded to 1024 bytes
+// as integers before, became offsets of the shared array (smem_align1024),
+// so its shared accesses compile to shared rather than generic loads and
+// stores: FP64 pipelined 49.6 / 45.8 us, FP32 pipelined 31.3 / 29.5 and,
+// storing the result from the registers (PP = 2: the tensor-copy unit
+// carries only the loads), 31.6 / 28.5 against 32.3 / 30.1 for the
+// load/store-unit kernel, so PP = 2 at 512 threads is the FP32 default.
 // fields: element type, bytes, log2 digit base, mode, sign, log2 L, log2 W,
 // threads, CTAs per SM, pipelined, default
 #define PAC_COLTMA_LIST(X)                                     \
@@ -162,8 +165,8 @@ namespace pac {
   /* pipelined, the result stored from the registers (PP = 2) */ \
   X(double, 8, 1, MODE_DIF, -1, 11, 2, 512, 1, 2, 0, 0)        \
   X(double, 8, 1, MODE_DIT, +1, 11, 2, 512, 1, 2, 0, 0)        \
-  X(float, 4, 1, MODE_DIF, -1, 11, 3, 512, 1, 2, 0, 0)         \
-  X(float, 4, 1, MODE_DIT, +1, 11, 3, 512, 1, 2, 0, 0)         \
+  X(float, 4, 1, MODE_DIF, -1, 11, 3, 512, 1, 2, 1, 0)         \
+  X(float, 4, 1, MODE_DIT, +1, 11, 3, 512, 1, 2, 1, 0)         \
   X(float, 4, 1, MODE_DIF, -1, 11, 3, 1024, 1, 2, 0, 0)        \
   X(float, 4, 1, MODE_DIT, +1, 11, 3, 1024, 1, 2, 0, 0)        \
   /* tensor-core form: radix-16 steps on tcgen05 MMAs */         \

@@ -17,6 +17,14 @@ namespace pac {
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
 }
+// The first 1024-byte boundary at or after the start of dynamic shared memory
+// (tensor-copy destinations).  Offsetting the array itself, instead of
+// rounding its address as an integer, keeps the pointer known to be shared
+// memory, so accesses through it compile to shared loads and stores rather
+// than generic ones.
+__device__ __forceinline__ unsigned char* smem_align1024(unsigned char* raw) {
+  return raw + ((1024u - (smem_u32(raw) & 1023u)) & 1023u);
+}
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
                : "memory");
