@@ -26,7 +26,7 @@ namespace pac {
   X(double, 8, 1, MODE_CONV, 0, 11, 0, 0, 128, 4, 0, 4)          \
   X(double, 8, 1, MODE_DIF, -1, 11, 1, 2, 512, 1, 0, 4)          \
   X(double, 8, 1, MODE_DIT, +1, 11, 1, 2, 512, 1, 0, 4)          \
-  X(float, 4, 1, MODE_CONV, 0, 11, 0, 1, 256, 4, 0, 4)           \
+  X(float, 4, 1, MODE_CONV, 0, 11, 0, 0, 128, 7, 0, 4)           \
   X(float, 4, 1, MODE_DIF, -1, 11, 1, 3, 512, 1, 0, 4)           \
   X(float, 4, 1, MODE_DIT, +1, 11, 1, 3, 512, 1, 0, 4)           \
   /* 3D FP32: 256-point rows and columns (256^3, and the middle axis of */ \
@@ -46,13 +46,20 @@ namespace pac {
   X(float, 4, 1, MODE_CONV, 0, 12, 0, 1, 256, 3, 0, 4)           \
   X(double, 8, 1, MODE_CONV, 0, 12, 0, 0, 256, 2, 0, 4)          \
   /* further candidates (PAC_SPECIAL_VARIANT=k, tuner knob special = k): */ \
-  /* the fused 2048-point FP32 pass at three and two CTAs per SM; on */      \
-  /* 2048^2 four (64 registers, no spills) ran 33.2 us, three 34.9, two */   \
-  /* 37.2; the FP64 pass at five CTAs per SM spills 144 bytes and ran */    \
+  /* the fused 2048-point FP32 pass: one line per 128-thread CTA at */     \
+  /* seven CTAs per SM (72 registers) is the default: 2048 lines over */    \
+  /* 148 SMs are 13.8 lines per SM, so seven resident lines leave */         \
+  /* almost no idle last round where eight (four CTAs of two lines) */      \
+  /* leave 14%; on 2048^2 it ran 31.6 us against 34.3 for two lines per */  \
+  /* 256-thread CTA at four CTAs per SM (64 registers), eight one-line */    \
+  /* CTAs 32.5; two lines at three and two CTAs per SM ran 34.9 and */        \
+  /* 37.2.  The FP64 pass at five CTAs per SM spills 144 bytes and ran */   \
   /* 53.2 us against 47.2 at four, and with two lines per 256-thread CTA */  \
   /* (two CTAs per SM) 51.4 against 46.5 */                                  \
+  X(float, 4, 1, MODE_CONV, 0, 11, 0, 1, 256, 4, 0, 4)           \
   X(float, 4, 1, MODE_CONV, 0, 11, 0, 1, 256, 3, 0, 4)           \
   X(float, 4, 1, MODE_CONV, 0, 11, 0, 1, 256, 2, 0, 4)           \
+  X(float, 4, 1, MODE_CONV, 0, 11, 0, 0, 128, 8, 0, 4)           \
   /* the 3D passes at the other occupancy: on 512 x 256 x 128 the */     \
   /* 512-point columns at 2 CTAs per SM ran 145 / 135 us against 149 / */ \
   /* 151 at one, the fused 128-point rows at 3 CTAs 155 against 160 us; */ \

@@ -430,6 +430,9 @@ TUNE_CANDIDATES = [
     {"max_factor_log": 0, "max_radix_log": 0, "special": 0, "w_shift": -1},
     {"max_factor_log": 0, "max_radix_log": 2, "special": 0, "w_shift": 2},
     {"max_factor_log": 0, "max_radix_log": 0, "special": 1, "w_shift": 0},
+    {"max_factor_log": 0, "max_radix_log": 0, "special": 2, "w_shift": 0},
+    {"max_factor_log": 0, "max_radix_log": 0, "special": 3, "w_shift": 0},
+    {"max_factor_log": 0, "max_radix_log": 0, "special": 4, "w_shift": 0},
 ]
 
 
