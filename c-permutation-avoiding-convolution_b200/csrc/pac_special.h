@@ -53,7 +53,8 @@ namespace pac {
   /* leave 14%; on 2048^2 it ran 31.6 us against 34.3 for two lines per */  \
   /* 256-thread CTA at four CTAs per SM (64 registers), eight one-line */    \
   /* CTAs 32.5; two lines at three and two CTAs per SM ran 34.9 and */        \
-  /* 37.2.  The FP64 pass at five CTAs per SM spills 144 bytes and ran */   \
+  /* 37.2.  The FP64 pass at three CTAs per SM ran 49.1 us against 45.9 */  \
+  /* at four; at five CTAs per SM it spills 144 bytes and ran */              \
   /* 53.2 us against 47.2 at four, and with two lines per 256-thread CTA */  \
   /* (two CTAs per SM) 51.4 against 46.5 */                                  \
   X(float, 4, 1, MODE_CONV, 0, 11, 0, 1, 256, 4, 0, 4)           \
@@ -69,11 +70,17 @@ namespace pac {
   X(float, 4, 1, MODE_DIT, +1, 9, 1, 4, 512, 1, 0, 4)            \
   X(float, 4, 1, MODE_CONV, 0, 7, 0, 5, 256, 2, 0, 4)            \
   /* tensor-core form, 2048-point rows and 8-line columns */             \
-  X(float, 4, 1, MODE_CONV, 0, 11, 0, 1, 256, 3, 1, 4)           \
+  X(float, 4, 1, MODE_CONV, 0, 11, 0, 0, 128, 5, 1, 4)           \
   X(float, 4, 1, MODE_DIF, -1, 11, 1, 3, 512, 1, 1, 4)           \
   X(float, 4, 1, MODE_DIT, +1, 11, 1, 3, 512, 1, 1, 4)           \
-  /* (three CTAs per SM, 80 registers: 58.6 us against 62.7 us at two) */ \
-  X(float, 4, 1, MODE_CONV, 0, 11, 0, 1, 256, 2, 1, 4)
+  /* (the fused pass with one line per 128-thread CTA at five CTAs per */ \
+  /* SM, 96 registers, ran 55.2 us against 59.1 for two lines per */       \
+  /* 256-thread CTA at three CTAs per SM (80 registers; 62.7 us at two), */ \
+  /* one line at seven CTAs per SM (72 registers, 12 bytes of spills) */   \
+  /* 55.6 us) */                                                             \
+  X(float, 4, 1, MODE_CONV, 0, 11, 0, 1, 256, 3, 1, 4)           \
+  X(float, 4, 1, MODE_CONV, 0, 11, 0, 1, 256, 2, 1, 4)           \
+  X(float, 4, 1, MODE_CONV, 0, 11, 0, 0, 128, 7, 1, 4)
 // Measured on C3 (2048^2): FP64 columns W=4 (32-byte rows) 53 us vs W=2
 // 68 us; FP32 columns W=8 34 us vs W=4 45 us -- row width, not occupancy,
 // bounds these passes (the narrower tiles were dropped from the list), and
