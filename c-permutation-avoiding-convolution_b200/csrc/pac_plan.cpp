@@ -659,16 +659,19 @@ static int run_transform(pac_plan_s* pl, const Schedule& s, int op, long long ba
 // The passes of one convolution call (2m - 1 for m factors): DIF over the
 // outer factors, the fused innermost pass, DIT back; all in place in y.
 // The plane schedule of a 3D convolution (pac_plane.cuh): the knob plane
-// (or, at its built-in 0, PAC_PLANE=1/0; unset: on for FP32 storage, off for
-// FP64), one factor per axis, the default radix schedules, and a plane
-// kernel compiled for the (N1, N2) planes.  Measured on FP32 256^3: 35% fewer
-// DRAM bytes per convolution and the same time as the line schedule; on
-// 512 x 256 x 128: 13% faster.
+// (or, at its built-in 0, PAC_PLANE=1/0; unset: off), one factor per axis,
+// the default radix schedules, and a plane kernel compiled for the (N1, N2)
+// planes.  Measured on FP32 256^3: 35% fewer DRAM bytes per convolution;
+// against the line schedule with load/store-unit column passes the same
+// time (and 13% faster on 512 x 256 x 128), but with the tensor-copy column
+// passes the line schedule is faster on both (0.297 against 0.345 ms, 0.333
+// against 0.350 ms), so it is the built-in choice and the tuner may still
+// pick the plane schedule.
 static bool plane_active(const Schedule& s, int* logC = nullptr, int* nt = nullptr) {
   int want = s.plane;
   if (want == 0) {
     const char* e = getenv("PAC_PLANE");
-    want = e ? (atoi(e) ? 1 : -1) : (s.bytes == 4 ? 1 : -1);
+    want = e ? (atoi(e) ? 1 : -1) : -1;
   }
   if (want <= 0 || s.tc || s.rlog_cap < 4 || s.vax.size() != 3) return false;
   for (int i = 0; i < 3; ++i)

@@ -183,6 +183,19 @@ namespace pac {
   X(float, 4, 1, MODE_DIT, +1, 11, 3, 512, 1, 2, 1, 0)         \
   X(float, 4, 1, MODE_DIF, -1, 11, 3, 1024, 1, 2, 0, 0)        \
   X(float, 4, 1, MODE_DIT, +1, 11, 3, 1024, 1, 2, 0, 0)        \
+  /* 3D FP32: 256- and 512-point columns of 16 lines (64-byte rows), */ \
+  /* pipelined at three (256) and two (512) CTAs per SM.  On 256^3 (line */ \
+  /* schedule) the four column passes took 59 / 51 / 54 / 51 us with */     \
+  /* tensor stores (the default), 59 / 53 / 53 / 53 with direct stores, */  \
+  /* against 75 / 70 / 73 / 72 for the load/store-unit kernel */            \
+  X(float, 4, 1, MODE_DIF, -1, 8, 4, 256, 3, 2, 0, 0)          \
+  X(float, 4, 1, MODE_DIT, +1, 8, 4, 256, 3, 2, 0, 0)          \
+  X(float, 4, 1, MODE_DIF, -1, 8, 4, 256, 3, 1, 1, 0)          \
+  X(float, 4, 1, MODE_DIT, +1, 8, 4, 256, 3, 1, 1, 0)          \
+  X(float, 4, 1, MODE_DIF, -1, 9, 4, 512, 2, 2, 0, 0)          \
+  X(float, 4, 1, MODE_DIT, +1, 9, 4, 512, 2, 2, 0, 0)          \
+  X(float, 4, 1, MODE_DIF, -1, 9, 4, 512, 2, 1, 1, 0)          \
+  X(float, 4, 1, MODE_DIT, +1, 9, 4, 512, 2, 1, 1, 0)          \
   /* tensor-core form: radix-16 steps on tcgen05 MMAs */         \
   X(float, 4, 1, MODE_DIF, -1, 11, 3, 512, 1, 0, 0, 1)         \
   X(float, 4, 1, MODE_DIT, +1, 11, 3, 512, 1, 0, 0, 1)

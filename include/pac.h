@@ -90,7 +90,8 @@ enum {
  *   plane           3D convolutions: 1 runs axes 1 and 2 of every plane in
  *                   one pass on a thread-block cluster (3 passes over HBM in
  *                   all) where a plane kernel exists for the shape, -1 the
- *                   line schedule (5 passes), 0 the built-in choice
+ *                   line schedule (5 passes), 0 the built-in choice (the
+ *                   line schedule, unless PAC_PLANE=1)
  * No counterpart in the reference, which has one fixed schedule per radix. */
 typedef struct {
   int max_factor_log;

@@ -177,6 +177,15 @@ def test_column_kernels(emu, orc, monkeypatch, form, kind):
     P.check_column_kernels(emu, orc, (2048, 32), 2, form, monkeypatch, kind)
 
 
+@pytest.mark.parametrize("kind", ["tile", "tma1", "tma2"])
+@pytest.mark.parametrize("dims", [(256, 32), (512, 32), (4, 256, 16)])
+def test_column_kernels_short(emu, orc, monkeypatch, dims, kind):
+    """256- and 512-point FP32 column passes of 16-line tiles (the 3D axes)
+    through the tensor-copy kernels: pipelined with direct stores (tma1)
+    and with tensor stores (tma2)."""
+    P.check_column_kernels(emu, orc, dims, 1, 1, monkeypatch, kind)
+
+
 @pytest.mark.parametrize("dims,batch", [((2048, 32), 2), ((2048, 8), 1)])
 def test_tc_tcgen05_columns(emu, orc, monkeypatch, dims, batch):
     """Tensor-core form with the column passes' radix-16 steps on tcgen05

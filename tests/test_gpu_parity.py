@@ -299,6 +299,22 @@ def test_column_kernels(lib, orc, monkeypatch, form, kind):
 
 
 
+@pytest.mark.parametrize("kind", ["tile", "tma1", "tma2"])
+@pytest.mark.parametrize("dims", [(256, 32), (512, 32), (4, 256, 16), (256, 256, 256),
+                                  (512, 256, 128)])
+def test_column_kernels_short(lib, orc, monkeypatch, dims, kind):
+    """256- and 512-point FP32 column passes of 16-line tiles (the 3D axes)
+    through the tensor-copy kernels, at the C4 sizes too."""
+    if np.prod(dims) > 2 ** 20:
+        monkeypatch.setenv("PAC_PLANE", "0")  # every axis as column passes
+        monkeypatch.setenv("PAC_COLTMA", "0" if kind == "tile" else kind[3:])
+        x, h = W.c4(dims)
+        y = P.native_conv(lib, dims, 1, 2, pac.PAC_FORM_F32, x, h)[0]
+        assert P.crel(y, P.fftconv(x, h, (0, 1, 2))) < P.TOL_F32
+        return
+    P.check_column_kernels(lib, orc, dims, 1, 1, monkeypatch, kind)
+
+
 @pytest.mark.parametrize("dims,batch", [((2048, 32), 2), ((2048, 256), 1), ((2048, 2048), 1)])
 def test_tc_tcgen05_columns(lib, orc, monkeypatch, dims, batch):
     """Tensor-core form with the column passes' radix-16 steps on tcgen05
