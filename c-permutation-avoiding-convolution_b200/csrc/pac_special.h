@@ -31,12 +31,15 @@ namespace pac {
   X(float, 4, 1, MODE_DIT, +1, 11, 1, 3, 512, 1, 0, 4)           \
   /* 3D FP32: 256-point rows and columns (256^3, and the middle axis of */ \
   /* 512 x 256 x 128), 512-point columns and 128-point rows */           \
-  X(float, 4, 1, MODE_CONV, 0, 8, 0, 4, 256, 3, 0, 4)            \
+  X(float, 4, 1, MODE_CONV, 0, 8, 0, 3, 128, 6, 0, 4)            \
   X(float, 4, 1, MODE_DIF, -1, 8, 1, 4, 256, 2, 0, 4)            \
   X(float, 4, 1, MODE_DIT, +1, 8, 1, 4, 256, 2, 0, 4)            \
   X(float, 4, 1, MODE_DIF, -1, 9, 1, 4, 512, 2, 0, 4)            \
   X(float, 4, 1, MODE_DIT, +1, 9, 1, 4, 512, 2, 0, 4)            \
   X(float, 4, 1, MODE_CONV, 0, 7, 0, 5, 256, 3, 0, 4)            \
+  /* 3D FP64: fused 256- and 128-point rows */                          \
+  X(double, 8, 1, MODE_CONV, 0, 8, 0, 3, 128, 4, 0, 4)           \
+  X(double, 8, 1, MODE_CONV, 0, 7, 0, 4, 128, 4, 0, 4)           \
   /* 1D batches: 16-point columns (one radix-16 stage, no shared memory) */ \
   X(float, 4, 1, MODE_DIF, -1, 4, 1, 8, 256, 4, 0, 4)            \
   X(float, 4, 1, MODE_DIT, +1, 4, 1, 8, 256, 4, 0, 4)            \
@@ -65,7 +68,19 @@ namespace pac {
   /* 512-point columns at 2 CTAs per SM ran 145 / 135 us against 149 / */ \
   /* 151 at one, the fused 128-point rows at 3 CTAs 155 against 160 us; */ \
   /* 256-point columns at 3 CTAs were 2-7% slower (not kept) */           \
+  /* the fused 256-point rows: FP32 eight lines per 128-thread CTA at */  \
+  /* six CTAs per SM (the default) ran 89.5 us on 256^3, sixteen lines */    \
+  /* per 256-thread CTA at three 97.6, at two 106.5, eight lines at */       \
+  /* eight CTAs 96.9; FP64 eight lines per 128-thread CTA at four CTAs */   \
+  /* (the default) 134 us, sixteen per 256-thread CTA at two 153 (the */     \
+  /* generic kernel took 254) */                                             \
+  X(float, 4, 1, MODE_CONV, 0, 8, 0, 4, 256, 3, 0, 4)            \
   X(float, 4, 1, MODE_CONV, 0, 8, 0, 4, 256, 2, 0, 4)            \
+  X(float, 4, 1, MODE_CONV, 0, 8, 0, 3, 128, 8, 0, 4)            \
+  X(double, 8, 1, MODE_CONV, 0, 8, 0, 4, 256, 2, 0, 4)           \
+  /* the fused 128-point FP32 rows at sixteen lines per 128-thread CTA */  \
+  X(float, 4, 1, MODE_CONV, 0, 7, 0, 4, 128, 6, 0, 4)            \
+  X(float, 4, 1, MODE_CONV, 0, 7, 0, 4, 128, 8, 0, 4)            \
   X(float, 4, 1, MODE_DIF, -1, 9, 1, 4, 512, 1, 0, 4)            \
   X(float, 4, 1, MODE_DIT, +1, 9, 1, 4, 512, 1, 0, 4)            \
   X(float, 4, 1, MODE_CONV, 0, 7, 0, 5, 256, 2, 0, 4)            \
@@ -196,6 +211,17 @@ namespace pac {
   X(float, 4, 1, MODE_DIT, +1, 9, 4, 512, 2, 2, 0, 0)          \
   X(float, 4, 1, MODE_DIF, -1, 9, 4, 512, 2, 1, 1, 0)          \
   X(float, 4, 1, MODE_DIT, +1, 9, 4, 512, 2, 1, 1, 0)          \
+  /* 3D FP64: 256- and 512-point columns of 8 lines (64-byte rows) */ \
+  /* (on 256^3 98-112 against 183-193 us per pass for the */        \
+  /* load/store-unit kernel; direct stores 100-138 us) */                \
+  X(double, 8, 1, MODE_DIF, -1, 8, 3, 128, 3, 1, 1, 0)         \
+  X(double, 8, 1, MODE_DIT, +1, 8, 3, 128, 3, 1, 1, 0)         \
+  X(double, 8, 1, MODE_DIF, -1, 9, 3, 256, 2, 1, 1, 0)         \
+  X(double, 8, 1, MODE_DIT, +1, 9, 3, 256, 2, 1, 1, 0)         \
+  X(double, 8, 1, MODE_DIF, -1, 8, 3, 128, 3, 2, 0, 0)         \
+  X(double, 8, 1, MODE_DIT, +1, 8, 3, 128, 3, 2, 0, 0)         \
+  X(double, 8, 1, MODE_DIF, -1, 9, 3, 256, 2, 2, 0, 0)         \
+  X(double, 8, 1, MODE_DIT, +1, 9, 3, 256, 2, 2, 0, 0)         \
   /* tensor-core form: radix-16 steps on tcgen05 MMAs */         \
   X(float, 4, 1, MODE_DIF, -1, 11, 3, 512, 1, 0, 0, 1)         \
   X(float, 4, 1, MODE_DIT, +1, 11, 3, 512, 1, 0, 0, 1)

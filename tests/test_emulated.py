@@ -45,7 +45,8 @@ def test_multi_factor_splits(emu, orc, cap, monkeypatch):
     # 512-point columns and 128-point rows, base-4 4096-point rows and
     # 16-point columns
     ((256, 16, 256), 1, 2, 1, False), ((256, 8, 256), 1, 2, 0, False),
-    ((512, 2, 128), 1, 2, 1, False), ((2 ** 16,), 2, 4, 0, False), ((2 ** 16,), 2, 4, 1, False),
+    ((512, 2, 128), 1, 2, 1, False), ((512, 2, 128), 1, 2, 0, False),
+    ((2 ** 16,), 2, 4, 0, False), ((2 ** 16,), 2, 4, 1, False),
     # fused 4096-point rows (FP64 one line per CTA, FP32 two); 16-point
     # columns of 256-column tiles (2^16 = 16 x 4096, a 16 x 8192 plane)
     ((4096,), 2, 2, 0, False), ((4096,), 4, 2, 1, True), ((16, 4096), 2, 2, 1, False),
@@ -179,11 +180,12 @@ def test_column_kernels(emu, orc, monkeypatch, form, kind):
 
 @pytest.mark.parametrize("kind", ["tile", "tma1", "tma2"])
 @pytest.mark.parametrize("dims", [(256, 32), (512, 32), (4, 256, 16)])
-def test_column_kernels_short(emu, orc, monkeypatch, dims, kind):
-    """256- and 512-point FP32 column passes of 16-line tiles (the 3D axes)
-    through the tensor-copy kernels: pipelined with direct stores (tma1)
-    and with tensor stores (tma2)."""
-    P.check_column_kernels(emu, orc, dims, 1, 1, monkeypatch, kind)
+@pytest.mark.parametrize("form", [0, 1])
+def test_column_kernels_short(emu, orc, monkeypatch, dims, kind, form):
+    """256- and 512-point column passes of 64-byte rows (16 FP32 or 8 FP64
+    lines; the 3D axes) through the pipelined tensor-copy kernels, with
+    tensor stores and with direct stores (tma1 / tma2)."""
+    P.check_column_kernels(emu, orc, dims, 1, form, monkeypatch, kind)
 
 
 @pytest.mark.parametrize("dims,batch", [((2048, 32), 2), ((2048, 8), 1)])

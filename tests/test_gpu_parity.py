@@ -191,7 +191,8 @@ def test_c5_full_batch(lib, orc):
     # 512-point columns and 128-point rows, base-4 4096-point rows and
     # 16-point columns
     ((256, 16, 256), 1, 2, 1, False), ((256, 8, 256), 1, 2, 0, False),
-    ((512, 2, 128), 1, 2, 1, False), ((2 ** 16,), 2, 4, 0, False), ((2 ** 16,), 2, 4, 1, False),
+    ((512, 2, 128), 1, 2, 1, False), ((512, 2, 128), 1, 2, 0, False),
+    ((2 ** 16,), 2, 4, 0, False), ((2 ** 16,), 2, 4, 1, False),
     ((2 ** 20,), 2, 2, 0, False), ((2 ** 20,), 2, 2, 1, False),
     # fused 4096-point rows (FP64 one line per CTA, FP32 two); 16-point
     # columns of 256-column tiles (2^16 = 16 x 4096, a 16 x 8192 plane)
@@ -302,17 +303,20 @@ def test_column_kernels(lib, orc, monkeypatch, form, kind):
 @pytest.mark.parametrize("kind", ["tile", "tma1", "tma2"])
 @pytest.mark.parametrize("dims", [(256, 32), (512, 32), (4, 256, 16), (256, 256, 256),
                                   (512, 256, 128)])
-def test_column_kernels_short(lib, orc, monkeypatch, dims, kind):
-    """256- and 512-point FP32 column passes of 16-line tiles (the 3D axes)
-    through the tensor-copy kernels, at the C4 sizes too."""
+@pytest.mark.parametrize("form", [0, 1])
+def test_column_kernels_short(lib, orc, monkeypatch, dims, kind, form):
+    """256- and 512-point column passes of 64-byte rows (16 FP32 or 8 FP64
+    lines; the 3D axes) through the pipelined tensor-copy kernels, at the
+    C4 sizes too."""
     if np.prod(dims) > 2 ** 20:
         monkeypatch.setenv("PAC_PLANE", "0")  # every axis as column passes
         monkeypatch.setenv("PAC_COLTMA", "0" if kind == "tile" else kind[3:])
         x, h = W.c4(dims)
-        y = P.native_conv(lib, dims, 1, 2, pac.PAC_FORM_F32, x, h)[0]
-        assert P.crel(y, P.fftconv(x, h, (0, 1, 2))) < P.TOL_F32
+        y = P.native_conv(lib, dims, 1, 2, form, x, h)[0]
+        tol = P.TOL if form == pac.PAC_FORM_F64 else P.TOL_F32
+        assert P.crel(y, P.fftconv(x, h, (0, 1, 2))) < tol
         return
-    P.check_column_kernels(lib, orc, dims, 1, 1, monkeypatch, kind)
+    P.check_column_kernels(lib, orc, dims, 1, form, monkeypatch, kind)
 
 
 @pytest.mark.parametrize("dims,batch", [((2048, 32), 2), ((2048, 256), 1), ((2048, 2048), 1)])
