@@ -36,7 +36,7 @@ namespace pac {
   X(float, 4, 1, MODE_DIT, +1, 8, 1, 4, 256, 2, 0, 4)            \
   X(float, 4, 1, MODE_DIF, -1, 9, 1, 4, 512, 2, 0, 4)            \
   X(float, 4, 1, MODE_DIT, +1, 9, 1, 4, 512, 2, 0, 4)            \
-  X(float, 4, 1, MODE_CONV, 0, 7, 0, 5, 256, 3, 0, 4)            \
+  X(float, 4, 1, MODE_CONV, 0, 7, 0, 4, 128, 8, 0, 4)            \
   /* 3D FP64: fused 256- and 128-point rows */                          \
   X(double, 8, 1, MODE_CONV, 0, 8, 0, 3, 128, 4, 0, 4)           \
   X(double, 8, 1, MODE_CONV, 0, 7, 0, 4, 128, 4, 0, 4)           \
@@ -78,9 +78,11 @@ namespace pac {
   X(float, 4, 1, MODE_CONV, 0, 8, 0, 4, 256, 2, 0, 4)            \
   X(float, 4, 1, MODE_CONV, 0, 8, 0, 3, 128, 8, 0, 4)            \
   X(double, 8, 1, MODE_CONV, 0, 8, 0, 4, 256, 2, 0, 4)           \
-  /* the fused 128-point FP32 rows at sixteen lines per 128-thread CTA */  \
+  /* the fused 128-point FP32 rows: sixteen lines per 128-thread CTA at */ \
+  /* eight CTAs per SM (the default) 107.1 us on 512 x 256 x 128, at six */  \
+  /* 109.3, thirty-two lines per 256-thread CTA at three 118.4 */            \
+  X(float, 4, 1, MODE_CONV, 0, 7, 0, 5, 256, 3, 0, 4)            \
   X(float, 4, 1, MODE_CONV, 0, 7, 0, 4, 128, 6, 0, 4)            \
-  X(float, 4, 1, MODE_CONV, 0, 7, 0, 4, 128, 8, 0, 4)            \
   X(float, 4, 1, MODE_DIF, -1, 9, 1, 4, 512, 1, 0, 4)            \
   X(float, 4, 1, MODE_DIT, +1, 9, 1, 4, 512, 1, 0, 4)            \
   X(float, 4, 1, MODE_CONV, 0, 7, 0, 5, 256, 2, 0, 4)            \
