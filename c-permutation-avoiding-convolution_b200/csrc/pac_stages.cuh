@@ -28,6 +28,30 @@ enum { IO_SMEM = 0, IO_GLOBAL = 1 };
 PAC_HDC bool col_pad32(int bytes, int cols, int W) { return bytes == 4 && cols == 1 && W == 8; }
 PAC_HD int sidx_col32(int e) { return e + (e >> 3) + 8 * (e >> 7); }
 
+// FP32 row tiles of 256-point lines (2 <= W <= 16) pad every line by one element
+// per 16 and start each line 16 banks after the previous one (pitch 272):
+// both radix-16 stages give a warp 16 butterflies of each of two lines --
+// 16 consecutive elements per line (j + 16m) in the outer stage, a stride of
+// 16 (16 blk + m) in the inner one -- and with this pad and pitch the two
+// lines fall on complementary halves of the 32 banks in both, where the
+// one-per-32 pad left every access 2-way conflicted.  (Not for the plane
+// pass's 32-row tiles, whose transposed stages read 32 consecutive columns
+// of a row and keep the one-per-32 pad.)
+PAC_HDC bool row_pad16(int bytes, int cols, int logL, int W) {
+  return bytes == 4 && cols == 0 && logL == 8 && W >= 2 && W <= 16;
+}
+PAC_HD int sidx_row16(int e) { return e + (e >> 4); }
+
+// FP32 row tiles of 128-point lines (2 <= W <= 16): the radix-16 stage gives
+// a warp 8 butterflies of each of four lines (j + 8m), the radix-8 stage 16
+// of each of two lines (8 blk + m).  Lines of pitch 136 with the one-per-32
+// pad, and bit 2 of the element index flipped in odd lines, put every such
+// access on 32 distinct banks (the pitch alone left the first stage 4-way
+// conflicted; no pitch does better than 2-way without the flip).
+PAC_HDC bool row_swz128(int bytes, int cols, int logL, int W) {
+  return bytes == 4 && cols == 0 && logL == 7 && W >= 2 && W <= 16;
+}
+
 // geometry policy; -1 = read from the PassDesc at run time.  TCL_ = 1: a
 // tile of the tensor-core form, whose column tiles keep the one-per-32 pad
 // (pitch_for gives them an odd pitch instead of sidx_col32).  TR_ = 1: the
@@ -72,6 +96,10 @@ struct Shape {
       return e * pitch(d) + sidx<T>(w);
     else if constexpr (!TCL_ && col_pad32((int)sizeof(T), COLS_, LOGW_ >= 0 ? 1 << LOGW_ : 0))
       return w * pitch(d) + sidx_col32(e);
+    else if constexpr (!TCL_ && row_pad16((int)sizeof(T), COLS_, LOGL_, LOGW_ >= 0 ? 1 << LOGW_ : 0))
+      return w * pitch(d) + sidx_row16(e);
+    else if constexpr (!TCL_ && row_swz128((int)sizeof(T), COLS_, LOGL_, LOGW_ >= 0 ? 1 << LOGW_ : 0))
+      return w * pitch(d) + sidx<T>(e ^ ((w & 1) << 2));
     else
       return w * pitch(d) + sidx<T>(e);
   }
@@ -889,6 +917,8 @@ PAC_HDC int pitch_for(int bytes, int logL, int W, int cols = 0, int tc = 0) {
     const int p = L + (L >> SH);
     return p + ((1 - p % NB) % NB + NB) % NB;
   }
+  if (!tc && row_pad16(bytes, cols, logL, W)) return L + (L >> 4);
+  if (!tc && row_swz128(bytes, cols, logL, W)) return L + (L >> 5) + 4;
   int pitch = !tc && col_pad32(bytes, cols, W) ? L + (L >> 3) + 8 * (L >> 7) : L + (L >> SH);
   if (W > 1) {
     int want = (NB / (W < NB ? W : NB)) % NB;
