@@ -78,6 +78,9 @@ namespace pac {
   X(float, 4, 1, MODE_CONV, 0, 8, 0, 4, 256, 2, 0, 4)            \
   X(float, 4, 1, MODE_CONV, 0, 8, 0, 3, 128, 8, 0, 4)            \
   X(double, 8, 1, MODE_CONV, 0, 8, 0, 4, 256, 2, 0, 4)           \
+  /* the fused 4096-point FP32 rows at one line per 256-thread CTA */   \
+  X(float, 4, 1, MODE_CONV, 0, 12, 0, 0, 256, 4, 0, 4)           \
+  X(float, 4, 1, MODE_CONV, 0, 12, 0, 0, 256, 3, 0, 4)           \
   /* the fused 128-point FP32 rows: sixteen lines per 128-thread CTA at */ \
   /* eight CTAs per SM (the default) 107.1 us on 512 x 256 x 128, at six */  \
   /* 109.3, thirty-two lines per 256-thread CTA at three 118.4 */            \

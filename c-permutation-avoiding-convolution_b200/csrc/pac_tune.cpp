@@ -252,7 +252,7 @@ static void descend(M measure, bool search_special, int bytes, pac_tune_result_t
   };
   if (search_special) {
     const pac_tune_t base = cur;
-    for (int sp : {-1, 1}) {  // generic kernels only; the second specialised candidates
+    for (int sp : {-1, 1, 2, 3, 4}) {  // generic kernels only; the k-th specialised candidates
       pac_tune_t t = base;
       t.special = sp;
       consider(t, false);

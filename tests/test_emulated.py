@@ -279,7 +279,7 @@ def test_tc_multi(emu):
 @pytest.mark.parametrize("tune", P.TUNE_CANDIDATES)
 @pytest.mark.parametrize("dims,batch,base,form", [
     ((4096,), 2, 2, 0), ((64, 2048), 1, 2, 1), ((2048, 32), 1, 2, 2), ((4096,), 1, 4, 1),
-    ((16, 32, 64), 2, 2, 0), ((2048, 64), 1, 2, 0), ((32, 2048), 1, 2, 0)])
+    ((16, 32, 64), 2, 2, 0), ((2048, 64), 1, 2, 0), ((32, 2048), 1, 2, 0), ((4096,), 2, 2, 1)])
 def test_tuned_plans(emu, dims, batch, base, form, tune):
     P.check_tuned(emu, dims, batch, base, form, tune)
 
