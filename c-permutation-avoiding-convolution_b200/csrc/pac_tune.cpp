@@ -4,9 +4,10 @@
 // the tuner allocates (contents irrelevant to the time: zeros), one plan per
 // candidate knob set, each timed with device events as the best of three
 // rounds of enough calls to fill ~10 ms.  The search is a coordinate
-// descent from the built-in knobs over (specialised kernels off or their
-// second candidates, radix 8 stages, shorter factors, narrower / wider
-// generic tiles); a step is kept
+// descent from the built-in knobs over (radix 8 stages, the plane or line
+// schedule of 3D problems, shorter factors, then -- once the factors that
+// the kernels serve are fixed -- specialised kernels off or their second to
+// fifth candidates, and narrower / wider generic tiles); a step is kept
 // only if it is at least 2% faster, so timing noise does not move a plan
 // off the built-in choices.  Candidates that build the same schedule as one
 // already timed (a factor cap that splits no axis differently) are skipped.
@@ -250,14 +251,6 @@ static void descend(M measure, bool search_special, int bytes, pac_tune_result_t
     }
     return false;
   };
-  if (search_special) {
-    const pac_tune_t base = cur;
-    for (int sp : {-1, 1, 2, 3, 4}) {  // generic kernels only; the k-th specialised candidates
-      pac_tune_t t = base;
-      t.special = sp;
-      consider(t, false);
-    }
-  }
   {
     pac_tune_t t = cur;
     t.max_radix_log = 3;
@@ -279,6 +272,15 @@ static void descend(M measure, bool search_special, int bytes, pac_tune_result_t
       pac_tune_t t = base;
       t.max_factor_log = c;
       consider(t, true);
+    }
+  }
+  // the kernel candidates after the factor split, whose geometries they serve
+  if (search_special) {
+    const pac_tune_t base = cur;
+    for (int sp : {-1, 1, 2, 3, 4}) {  // generic kernels only; the k-th specialised candidates
+      pac_tune_t t = base;
+      t.special = sp;
+      consider(t, false);
     }
   }
   {

@@ -426,7 +426,8 @@ def test_c4_3d_tc(lib, shape):
 @pytest.mark.parametrize("tune", P.TUNE_CANDIDATES)
 @pytest.mark.parametrize("dims,batch,base,form", [
     ((2048, 2048), 1, 2, 1), ((65536,), 4, 2, 0), ((256, 256, 256), 1, 2, 1),
-    ((64, 2048), 2, 2, 2), ((4096,), 3, 4, 0), ((65536,), 2, 2, 1)])
+    ((64, 2048), 2, 2, 2), ((4096,), 3, 4, 0), ((65536,), 2, 2, 1),
+    ((4096,), 2, 2, 1)])
 def test_tuned_plans(lib, dims, batch, base, form, tune):
     P.check_tuned(lib, dims, batch, base, form, tune)
 
