@@ -522,7 +522,13 @@ int be_l2_persist(void* stream, const void* base, size_t bytes) {
   }
   PAC_CU(cudaStreamSetAttribute((cudaStream_t)stream, cudaStreamAttributeAccessPolicyWindow, &v),
          "cudaStreamSetAttribute");
-  if (bytes == 0) cudaCtxResetPersistingL2Cache();
+  if (bytes == 0) {
+    // back to no set-aside: persisting lines become normal lines and the
+    // whole L2 serves normal accesses again
+    cudaCtxResetPersistingL2Cache();
+    if (prop.persistingL2CacheMaxSize > 0)
+      PAC_CU(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, 0), "cudaDeviceSetLimit");
+  }
   return PAC_SUCCESS;
 }
 
