@@ -52,24 +52,6 @@ PAC_HDC bool row_swz128(int bytes, int cols, int logL, int W) {
   return bytes == 4 && cols == 0 && logL == 7 && W >= 2 && W <= 16;
 }
 
-// FP32 rows of 2048 points (schedule 16, 16, 8; a warp stays inside one
-// line): the radix-16 middle stage gives a warp 8 consecutive j in each of 4
-// blocks of 128 (128 blk + j + 8m), which the one-per-32 pad left 2-way
-// conflicted.  Flipping the low 5 bits of the element index by a linear map
-// of the higher bits x = e >> 5 -- bits 0-2 by x mod 8 (the innermost stage's
-// 32 consecutive blocks of 8), bits 3-4 by bits 2-3 of x (the middle stage's
-// block index) -- keeps every 32-aligned group a permutation (the outer
-// stage's 32 consecutive j) and puts all three stages on 32 distinct banks.
-// The line pitch keeps the generic pad, so the generic kernel's index stays
-// inside the same tile.
-PAC_HDC bool row_swz2048(int bytes, int cols, int logL) {
-  return bytes == 4 && cols == 0 && logL == 11;
-}
-PAC_HD int sidx_row2048(int e) {
-  const int x = e >> 5;
-  return e ^ ((x & 7) | (((x >> 2) & 3) << 3));
-}
-
 // FP32 columns of 512 points in 16-line tiles (schedule 8, 8, 8; pitch 546,
 // two banks per line): the middle stage gives a warp 8 consecutive j in each
 // of 4 blocks of 64 of one line (4-way conflicted with the one-per-32 pad),
@@ -133,8 +115,6 @@ struct Shape {
       return w * pitch(d) + sidx_row16(e);
     else if constexpr (!TCL_ && row_swz128((int)sizeof(T), COLS_, LOGL_, LOGW_ >= 0 ? 1 << LOGW_ : 0))
       return w * pitch(d) + sidx<T>(e ^ ((w & 1) << 2));
-    else if constexpr (!TCL_ && LOGW_ >= 0 && row_swz2048((int)sizeof(T), COLS_, LOGL_))
-      return w * pitch(d) + sidx_row2048(e);
     else if constexpr (!TCL_ && col_swz512((int)sizeof(T), COLS_, LOGL_, LOGW_ >= 0 ? 1 << LOGW_ : 0))
       return w * pitch(d) + sidx_col512(e);
     else
