@@ -6,7 +6,7 @@
 
 A step is one convolution of one batch of the configuration's synthetic
 input.  The default workload is C3: a 2D 2048 x 2048 complex FP64 circular
-convolution with a 31 x 31 Gaussian filter (the configuration the north-star
+convolution with a 31 x 31 Gaussian filter (the configuration the headline
 target is quoted on).  ``value`` times K steps of pac_convolve on
 device-resident data (CUDA events, inputs larger than L2, max over ranks);
 ``e2e`` times the reference-compatible call

@@ -7,7 +7,7 @@ import numpy as np
 
 from conftest import O, pac, rel_l2, rng
 
-TOL = 1e-13  # FP64 forms vs the FP64 oracle (north star: 1e-13 relative L2)
+TOL = 1e-13  # FP64 forms vs the FP64 oracle (relative L2)
 TOL_F32 = 1e-6  # FP32 form vs the FP64 oracle
 TOL_TC = 1e-6  # tensor-core form (split FP16 radix-16 stages) vs the FP64 oracle
 
