@@ -318,7 +318,7 @@ __global__ void __launch_bounds__(NT, MINB)
 // Tensor maps of a ColTma pass over the row array [O][L][S] of one
 // component: the dense rows (3D {S, L, O}, boxes of W x boxr rows) and the
 // transposed view (4D {S, L/R, R, O}: row e = blk * R + m, boxes of W x boxb
-// blocks x R) that lands as [m][blk][w].  Unswizzled; no multicast.
+// blocks x R) that lands as [m][blk][w].  Unswizzled; plain copies.
 static int coltma_map(CUtensorMap* m, const void* base, int esz, const PassDesc& d, int W,
                       int boxr, bool trans, int vin, int boxb) {
   auto enc = tensor_map_encoder();

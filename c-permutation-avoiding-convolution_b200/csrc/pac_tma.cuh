@@ -1,7 +1,7 @@
 // pac_tma.cuh -- tensor copies (TMA), bulk copies and mbarriers on sm_100a,
 // shared by the kernels of pac_cuda.cu and pac_coltma.cu.  Every load is a
-// plain (non-multicast) copy into this CTA's shared memory; every wait on an
-// mbarrier is bounded.
+// plain copy from this GPU's memory into this CTA's own shared memory; every
+// wait on an mbarrier is bounded.
 #pragma once
 
 #include <cudaTypedefs.h>
@@ -79,7 +79,7 @@ __device__ __forceinline__ void report_timeout(const PassDesc& d) {
   if (d.status) atomicExch(d.status, (int)PAC_ERROR_TIMEOUT);
 }
 // box {W, BOXR, 1} of a 3D tensor map at (c0, c1, c2) into shared memory;
-// completion counted on bar.  No multicast.
+// completion counted on bar; this CTA's shared memory only.
 __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar,
                                             int c0, int c1, int c2) {
   asm volatile(
@@ -91,7 +91,7 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, u
 __device__ __forceinline__ void fence_proxy_async() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
-// box of a 4D tensor map at (c0, c1, c2, c3) into shared memory; no multicast
+// box of a 4D tensor map at (c0, c1, c2, c3) into this CTA's shared memory
 __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, uint64_t* bar,
                                             int c0, int c1, int c2, int c3) {
   asm volatile(
